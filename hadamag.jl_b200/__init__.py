@@ -1,0 +1,309 @@
+"""hadamag_b200 -- HadaMAG.jl's exact-SRE / MC_SRE / Mana hot path on NVIDIA B200.
+
+Python mirror of the reference's user API (src/HadaMAG.jl:1-25): the same names,
+argument meanings and error behaviour, served by one backend, ``:b200``, which calls
+libhadamag_b200.so (hand-written sm_100a kernels behind a C ABI, see
+include/hadamag_b200.h).  There is no CPU fallback: without the shared object or a
+CUDA device every compute call raises.
+
+    import hadamag_b200 as hm
+    psi = hm.StateVec(vec)              # vec: complex128, length 2^n
+    value, lost_norm = hm.SRE(psi, 2)   # src/SRE.jl:75-83
+    m2 = hm.MC_SRE(psi, 2, Nbeta=13, Nsamples=1000, seed=123)
+    mana = hm.Mana(hm.StateVec(v3, q=3))          # src/Mana.jl:15-17
+    mana_rho = hm.Mana(hm.DensityMatrix(rho, q=3))  # src/Mana.jl:305-314
+
+The package directory is ``hadamag.jl_b200/``; the repository root's
+``hadamag_b200.py`` makes it importable as ``hadamag_b200``.
+"""
+import os
+import warnings
+
+import numpy as np
+
+from ._native import (HM_FP32, HM_FP64, HM_PLAIN, PRECISIONS, ArgumentError, Context, HadaMAGError,
+                      default_context, load_library)
+
+__all__ = [
+    "StateVec", "DensityMatrix", "SRE", "MC_SRE", "Mana", "SRE_batched", "SRE_grad", "generate_gray_table",
+    "load_state", "reduced_density_matrix", "proposal_stream", "qubits", "qudits", "qudit_dim", "data",
+    "ArgumentError", "HadaMAGError", "Context", "B200",
+]
+
+
+# ----------------------------------------------------------------------------------
+# containers (src/State.jl:11-63, src/DensityMatrix.jl:8-41)
+
+def _power_q(length, q):
+    """(n, is_power) with length == q^n, as _power_q of src/Helpers.jl:7-15."""
+    n, tmp = 0, int(length)
+    while tmp > 0 and tmp % q == 0:
+        tmp //= q
+        n += 1
+    return n, tmp == 1
+
+
+class StateVec:
+    """Pure state of n q-dits; ``data`` is a complex128 vector of length q^n.
+
+    Raises ArgumentError when the length is not a power of q (src/State.jl:40-44).
+    """
+
+    def __init__(self, vec, q=2):
+        v = np.array(vec, dtype=np.complex128).reshape(-1)
+        n, ok = _power_q(v.size, q)
+        if not ok:
+            raise ArgumentError(f"length(vec)={v.size} is not a power of q={q}")
+        self.data, self.n, self.q = v, n, q
+
+    def __len__(self):
+        return self.data.size
+
+    def __repr__(self):
+        return f"StateVec{{ComplexF64,{self.q}}}(n={self.n}, dim={self.data.size})"
+
+    def normalize(self):
+        self.data /= np.linalg.norm(self.data)
+        return self
+
+
+class DensityMatrix:
+    """Mixed state of n q-dits; ``data`` is a complex128 q^n x q^n matrix.
+
+    Raises ArgumentError when the matrix is not square or its size is not a power of q
+    (src/DensityMatrix.jl:28-35).
+    """
+
+    def __init__(self, mat, q=2):
+        m = np.array(mat, dtype=np.complex128)
+        if m.ndim != 2 or m.shape[0] != m.shape[1]:
+            raise ArgumentError("DensityMatrix must be square")
+        n, ok = _power_q(m.shape[0], q)
+        if not ok:
+            raise ArgumentError(f"size(mat,1)={m.shape[0]} is not a power of q={q}")
+        self.data, self.n, self.q = m, n, q
+
+    def __repr__(self):
+        return f"DensityMatrix{{ComplexF64,{self.q}}}(n={self.n}, size={self.data.shape})"
+
+
+def qudits(s):
+    return s.n
+
+
+def qubits(s):
+    if s.q != 2:
+        raise ArgumentError("qubits() is defined for q = 2 states")
+    return s.n
+
+
+def qudit_dim(s):
+    return s.q
+
+
+def data(s):
+    return s.data
+
+
+# ----------------------------------------------------------------------------------
+# backend selection (src/Backends/Dispatch.jl:4-90)
+
+class B200:
+    """The sm_100a backend; ``device`` selects the CUDA device."""
+
+    def __init__(self, device=0):
+        self.device = device
+
+    def context(self):
+        return default_context(self.device)
+
+
+def _choose_backend(b, device=0):
+    """``:b200`` (or ``:auto`` / None, since it is the only backend of this package).
+
+    The reference's CPU, MPI and CUDA.jl backends live in HadaMAG.jl itself; asking this
+    package for them is an ArgumentError rather than a silent substitution.
+    """
+    if isinstance(b, B200):
+        return b
+    name = (b or "auto").lstrip(":") if isinstance(b, str) or b is None else str(b)
+    if name in ("b200", "auto"):
+        return B200(device)
+    raise ArgumentError(f"backend :{name} is provided by HadaMAG.jl; this package implements :b200")
+
+
+def _progress_warning(progress):
+    if progress:
+        warnings.warn("Progress bar not implemented for the b200 backend.", stacklevel=3)
+
+
+def _precision(p):
+    if isinstance(p, int):
+        return p
+    try:
+        return PRECISIONS[str(p).lower()]
+    except KeyError:
+        raise ArgumentError(f"precision must be one of {sorted(PRECISIONS)} (got {p!r})") from None
+
+
+def _as_state(psi, q):
+    if isinstance(psi, StateVec):
+        if psi.q != q:
+            raise ArgumentError(f"expected a StateVec with q={q}, got q={psi.q}")
+        return psi
+    return StateVec(psi, q=q)
+
+
+# ----------------------------------------------------------------------------------
+# user API
+
+def SRE(psi, q, backend="auto", progress=False, precision="fp64", device=0):
+    """Exact stabilizer Renyi entropy; returns (value, lost_norm).
+
+    value = -log2(sum_P <psi|P|psi>^(2q) / 2^n) over all 4^n Pauli strings and
+    lost_norm = |1 - sum_P <psi|P|psi>^2 / 2^n|, as src/SRE.jl:75-83 and
+    src/Backends/Threads.jl:263-314 (for q != 2 the value is (q-1) M_q, as there).
+    precision: "fp64" (default), "fp32" (FP32 butterflies, FP64 reductions) or "plain"
+    (the reference CUDA backend's multi-launch structure, FP64).
+    """
+    _progress_warning(progress)
+    be = _choose_backend(backend, device)
+    s = _as_state(psi, 2)
+    vals, lost = be.context().sre(s.data, (float(q),), _precision(precision))
+    return float(vals[0]), float(lost)
+
+
+def SRE_batched(psis, qs=(2,), precision="fp64", device=0):
+    """Exact SRE of many states (qubit counts may differ) in one launch sequence.
+
+    Returns (values[nstates, len(qs)], lost_norm[nstates]).  No reference counterpart.
+    """
+    states = [_as_state(p, 2).data for p in psis]
+    return default_context(device).sre_batched(states, tuple(float(q) for q in qs), _precision(precision))
+
+
+def SRE_grad(psi, q=2, device=0):
+    """Value and gradient of the exact SRE_q; grad.real = dSRE/dRe(psi), grad.imag =
+    dSRE/dIm(psi).  No reference counterpart (hand-written adjoint kernel)."""
+    s = _as_state(psi, 2)
+    return default_context(device).sre_grad(s.data, float(q))
+
+
+def proposal_stream(L, Nbeta, Nsamples, seed=None):
+    """Metropolis proposal stream with the distribution of src/SRE.jl:142-170.
+
+    Chain i (1-based) uses seed + i: tries[t] = floor(9 u) + 1 single-site flips with
+    sites uniform in 1..L, XOR-ed into prop_delta[t]; rs[t] uniform in [0, 1).  Julia's
+    MersenneTwister stream itself cannot be regenerated outside Julia; the Julia
+    backend passes the reference's own draws through the same C ABI.
+    """
+    base = int(np.random.default_rng().integers(1, 10**9)) if seed is None else int(seed)
+    pd = np.zeros((Nbeta, Nsamples), dtype=np.uint64)
+    rs = np.zeros((Nbeta, Nsamples), dtype=np.float64)
+    for i in range(Nbeta):
+        g = np.random.default_rng(base + i + 1)
+        u = g.random(Nsamples)
+        tries = np.floor(u * 9).astype(np.int64) + 1
+        rs[i] = g.random(Nsamples)
+        sites = g.integers(0, L, size=int(tries.sum()))
+        bits = (np.uint64(1) << sites.astype(np.uint64))
+        idx = np.repeat(np.arange(Nsamples), tries)
+        np.bitwise_xor.at(pd[i], idx, bits)
+    return pd, rs
+
+
+def MC_SRE(psi, q, backend="auto", Nbeta=13, Nsamples=1000, seed=None, progress=False, device=0,
+           prop_delta=None, rs=None):
+    """Monte-Carlo SRE_q (src/SRE.jl:33-43, src/Backends/Threads.jl:316-376).
+
+    Nbeta chains at beta_i = (i-1)/(Nbeta-1) (Nbeta odd, Simpson's rule); returns
+    -log2(2^-I + I_add).  The proposal stream comes from proposal_stream(seed) unless
+    given explicitly (prop_delta, rs with shape (Nbeta, Nsamples)).
+    """
+    _progress_warning(progress)
+    if Nbeta % 2 != 1:
+        raise ArgumentError("Simpson needs an odd number of β points.")
+    be = _choose_backend(backend, device)
+    s = _as_state(psi, 2)
+    if prop_delta is None or rs is None:
+        prop_delta, rs = proposal_stream(s.n, Nbeta, Nsamples, seed)
+    m2, _, _, _, _ = be.context().mc_sre(s.data, float(q), Nbeta, Nsamples, prop_delta, rs)
+    return m2
+
+
+def Mana(psi, backend="auto", progress=False, device=0):
+    """Mana of a qutrit state.
+
+    StateVec (q=3): log2(sum |W|) / log2(3) over the phase-space transforms of every
+    ternary X-string (src/Mana.jl:15-92, src/Backends/Threads.jl:378-426).
+    DensityMatrix (q=3): log2(sum |M^(x)N vec9(rho)| / 3^N) (src/Mana.jl:305-314).
+    """
+    _progress_warning(progress)
+    if isinstance(psi, DensityMatrix):
+        if psi.q != 3:
+            raise ArgumentError("Mana needs a qutrit DensityMatrix (q=3)")
+        return default_context(device).mana_mixed(psi.data)
+    be = _choose_backend(backend, device)
+    s = _as_state(psi, 3)
+    return be.context().mana_pure(s.data)
+
+
+def generate_gray_table(n, q):
+    """Gray table as src/Basis.jl:544-557, computed on the device.
+
+    q == 2: (codes uint64[2^n], flips int64[2^n - 1], 1-based).
+    q > 2:  (XTAB int64[n, q^n], flips int64[q^n - 1], 1-based).
+    """
+    if q < 2:
+        raise AssertionError("Base q must be ≥ 2")
+    ctx = default_context()
+    return ctx.gray_table(n) if q == 2 else ctx.gray_table_general(n, q)
+
+
+def load_state(path, q=2):
+    """StateVec from disk (src/State.jl:388-404): .npy (numpy), otherwise whitespace-
+    separated real/imaginary pairs.  .jld2 needs h5py, which this image does not ship."""
+    if path.endswith(".npy"):
+        return StateVec(np.load(path), q=q)
+    if path.endswith(".jld2"):
+        try:
+            import h5py  # noqa: F401
+        except ImportError:
+            raise ArgumentError(".jld2 states need h5py, which is not installed") from None
+        with h5py.File(path, "r") as f:
+            d = f["state"][()]
+        if d.dtype.names:
+            d = d[d.dtype.names[0]] + 1j * d[d.dtype.names[1]]
+        return StateVec(d, q=q)
+    with open(path) as f:
+        vals = [float(t) for t in f.read().split()]
+    if len(vals) % 2 != 0:
+        raise ArgumentError("File does not contain real/imaginary pairs")
+    v = np.array(vals[0::2]) + 1j * np.array(vals[1::2])
+    return StateVec(v, q=q)
+
+
+def reduced_density_matrix(psi, NA, side="right", q=None):
+    """rho_A = Tr_B |psi><psi| for a contiguous bipartition (src/DensityMatrix.jl:94-123).
+
+    side="right" keeps the NA most significant sites, side="left" the NA least
+    significant.  State preparation utility (host numpy), not part of the hot path.
+    """
+    s = psi if isinstance(psi, StateVec) else StateVec(psi, q=q or 2)
+    qq = s.q
+    if qq not in (2, 3):
+        raise ArgumentError("only q=2 and q=3 are implemented")
+    N = s.n
+    if not (0 <= NA <= N):
+        raise ArgumentError(f"need 0 ≤ NA ≤ N (got NA={NA}, N={N})")
+    dimA, dimB = qq ** NA, qq ** (N - NA)
+    v = s.data
+    if side == "left":
+        M = v.reshape(dimB, dimA).T          # M[iA, kB] = psi[iA + dimA kB]
+        rho = M @ M.conj().T
+    elif side == "right":
+        M = v.reshape(dimA, dimB)            # M[iA, kB] = psi[iA dimB + kB]
+        rho = M @ M.conj().T
+    else:
+        raise ArgumentError(f"side must be :left or :right (got {side})")
+    return DensityMatrix(rho, q=qq)

@@ -1,0 +1,124 @@
+// hm_ctx.h -- host-side context shared by the C-ABI and the launchers (not part of the ABI).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <string>
+
+#include "../../include/hadamag_b200.h"
+
+struct hm_ctx {
+  int device = 0;
+  int num_sms = 0;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  double last_ms = 0.0;
+  std::string err;
+
+  // grow-only device buffers
+  void *d_psi = nullptr;  // double2 copy of the input state
+  size_t psi_cap = 0;
+  void *d_psi32 = nullptr;  // float2 copy (FP32 path)
+  size_t psi32_cap = 0;
+  void *d_inter = nullptr;  // two-pass ring / plain-path column batch
+  size_t inter_cap = 0;
+  double *d_partials = nullptr;
+  size_t partials_cap = 0;
+  unsigned *d_ctrl = nullptr;  // queue + error flag + dependency counters
+  size_t ctrl_cap = 0;
+  double *d_out = nullptr;  // fold output
+  size_t out_cap = 0;
+  void *d_aux = nullptr;  // per-feature scratch (masks, Mana, MC state)
+  size_t aux_cap = 0;
+  void *d_aux2 = nullptr;
+  size_t aux2_cap = 0;
+  double *h_out = nullptr;  // pinned host mirror of d_out
+  size_t h_out_cap = 0;
+  void *h_pin = nullptr;  // pinned host scratch
+  size_t h_pin_cap = 0;
+};
+
+namespace hm {
+
+// error helpers: record the message on the context and return the status
+inline int set_err(hm_ctx *c, int code, const char *fmt, ...) __attribute__((format(printf, 3, 4)));
+inline int set_err(hm_ctx *c, int code, const char *fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof buf, fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define HM_CUDA(c, call)                                                                              \
+  do {                                                                                                \
+    cudaError_t e_ = (call);                                                                          \
+    if (e_ != cudaSuccess)                                                                            \
+      return ::hm::set_err((c), HM_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                           __FILE__, __LINE__);                                                       \
+  } while (0)
+
+#define HM_TRY(expr)          \
+  do {                        \
+    int rc_ = (expr);         \
+    if (rc_ != HM_OK) return rc_; \
+  } while (0)
+
+// grow-only device buffer
+inline int ensure_dev(hm_ctx *c, void **p, size_t *cap, size_t bytes) {
+  if (bytes <= *cap && *p) return HM_OK;
+  if (*p) {
+    cudaStreamSynchronize(c->stream);
+    cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+  }
+  size_t want = bytes < 256 ? 256 : bytes;
+  cudaError_t e = cudaMalloc(p, want);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return set_err(c, HM_ERR_OOM, "cudaMalloc(%zu) failed: %s", want, cudaGetErrorString(e));
+  }
+  *cap = want;
+  return HM_OK;
+}
+
+inline int ensure_host(hm_ctx *c, void **p, size_t *cap, size_t bytes) {
+  if (bytes <= *cap && *p) return HM_OK;
+  if (*p) {
+    cudaStreamSynchronize(c->stream);
+    cudaFreeHost(*p);
+    *p = nullptr;
+    *cap = 0;
+  }
+  size_t want = bytes < 256 ? 256 : bytes;
+  cudaError_t e = cudaMallocHost(p, want);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return set_err(c, HM_ERR_OOM, "cudaMallocHost(%zu) failed: %s", want, cudaGetErrorString(e));
+  }
+  *cap = want;
+  return HM_OK;
+}
+
+struct QReq {
+  double q[4];
+  int nq;
+};
+
+// exact SRE raw sums over Gray indices [kb, ke) of a device-resident double2 state.
+// out_dd (host): [p2_hi, p2_lo, m0_hi, m0_lo, ...] for each requested q.
+int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, const QReq &q, int precision,
+            double *out_dd);
+int run_sre_plain(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, const QReq &q,
+                  double *out_dd);
+
+}  // namespace hm

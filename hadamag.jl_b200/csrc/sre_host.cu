@@ -1,0 +1,139 @@
+// sre_host.cu -- exact-SRE driver: precision dispatch, fold of the per-warp partials,
+// result read-back.
+#include <math.h>
+
+#include "sre_launch.cuh"
+
+namespace hm {
+
+template <typename T, int R, int QS>
+int launch_sre_qs(hm_ctx *c, const void *psi_dev, int n, uint64_t kb, uint64_t ke, const QParams &qp, int *nwarps);
+
+template <typename T>
+static int launch_sre_prec(hm_ctx *c, const void *psi_dev, int n, uint64_t kb, uint64_t ke, int kind,
+                           const QParams &qp, int *nwarps) {
+  switch (kind) {
+    case QS_Q2:
+      return launch_sre_qs<T, 32, QS_Q2>(c, psi_dev, n, kb, ke, qp, nwarps);
+    case QS_Q23:
+      return launch_sre_qs<T, 32, QS_Q23>(c, psi_dev, n, kb, ke, qp, nwarps);
+    default:
+      return launch_sre_qs<T, 32, QS_GEN>(c, psi_dev, n, kb, ke, qp, nwarps);
+  }
+}
+
+TwoPassCfg &twopass_cfg() {
+  static TwoPassCfg cfg;
+  return cfg;
+}
+
+__global__ void k_fold_partials(const double *__restrict__ partials, int nwarps, int nsum, double *out) {
+  // one block; thread t folds warps t, t + blockDim, ... then a fixed-shape tree
+  __shared__ dd sh[256][5];
+  const int t = threadIdx.x;
+  dd acc[5];
+  for (int s = 0; s < 5; ++s) acc[s] = dd{0.0, 0.0};
+  for (int w = t; w < nwarps; w += blockDim.x)
+    for (int s = 0; s < nsum; ++s) {
+      dd v{partials[(size_t)w * 2 * nsum + 2 * s], partials[(size_t)w * 2 * nsum + 2 * s + 1]};
+      dd_add_dd(acc[s], v);
+    }
+  for (int s = 0; s < 5; ++s) sh[t][s] = acc[s];
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (t < o)
+      for (int s = 0; s < nsum; ++s) dd_add_dd(sh[t][s], sh[t + o][s]);
+    __syncthreads();
+  }
+  if (t == 0)
+    for (int s = 0; s < nsum; ++s) {
+      out[2 * s] = sh[0][s].hi;
+      out[2 * s + 1] = sh[0][s].lo;
+    }
+}
+
+__global__ void k_psi_to_f32(const double2 *__restrict__ in, float2 *__restrict__ out, uint64_t len) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < len; i += (uint64_t)gridDim.x * blockDim.x) {
+    const double2 v = in[i];
+    out[i] = make_float2((float)v.x, (float)v.y);
+  }
+}
+
+// Map requested q values onto a kernel moment set.  Returns the kind and, per request,
+// the index of its sum in the kernel output (1-based; 0 is sum F^2).
+static int choose_qs(const QReq &q, QParams &qp, int *idx) {
+  bool only23 = true, has3 = false;
+  for (int i = 0; i < q.nq; ++i) {
+    if (q.q[i] != 2.0 && q.q[i] != 3.0) only23 = false;
+    if (q.q[i] == 3.0) has3 = true;
+  }
+  memset(&qp, 0, sizeof qp);
+  if (only23 && !has3) {
+    for (int i = 0; i < q.nq; ++i) idx[i] = 1;
+    return QS_Q2;
+  }
+  if (only23) {
+    for (int i = 0; i < q.nq; ++i) idx[i] = q.q[i] == 2.0 ? 1 : 2;
+    return QS_Q23;
+  }
+  qp.nq = q.nq;
+  for (int i = 0; i < q.nq; ++i) {
+    qp.q[i] = q.q[i];
+    idx[i] = 1 + i;
+  }
+  for (int i = q.nq; i < 4; ++i) qp.q[i] = 2.0;
+  return QS_GEN;
+}
+
+int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, const QReq &q, int precision,
+            double *out_dd) {
+  if (precision == HM_PLAIN || n > 21 || n < 1) return run_sre_plain(c, psi_dev, n, kb, ke, q, out_dd);
+  if (ke <= kb) {
+    for (int i = 0; i < 2 * (1 + q.nq); ++i) out_dd[i] = 0.0;
+    return HM_OK;
+  }
+  QParams qp;
+  int idx[4];
+  const int kind = choose_qs(q, qp, idx);
+  const int nsum = 1 + (kind == QS_Q2 ? 1 : (kind == QS_Q23 ? 2 : 4));
+  const uint64_t len = 1ull << n;
+  const void *psi_k = psi_dev;
+  if (precision == HM_FP32) {
+    HM_TRY(ensure_dev(c, &c->d_psi32, &c->psi32_cap, len * sizeof(float2)));
+    k_psi_to_f32<<<c->num_sms * 4, 256, 0, c->stream>>>(psi_dev, (float2 *)c->d_psi32, len);
+    HM_CUDA(c, cudaGetLastError());
+    psi_k = c->d_psi32;
+  }
+  int nwarps = 0;
+  HM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+  if (precision == HM_FP32)
+    HM_TRY((launch_sre_prec<float>(c, psi_k, n, kb, ke, kind, qp, &nwarps)));
+  else
+    HM_TRY((launch_sre_prec<double>(c, psi_k, n, kb, ke, kind, qp, &nwarps)));
+  HM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+  HM_TRY(ensure_dev(c, (void **)&c->d_out, &c->out_cap, sizeof(double) * 16));
+  k_fold_partials<<<1, 256, 0, c->stream>>>(c->d_partials, nwarps, nsum, c->d_out);
+  HM_CUDA(c, cudaGetLastError());
+  HM_TRY(ensure_host(c, (void **)&c->h_out, &c->h_out_cap, sizeof(double) * 16 + 64));
+  HM_CUDA(c, cudaMemcpyAsync(c->h_out, c->d_out, sizeof(double) * 2 * nsum, cudaMemcpyDeviceToHost, c->stream));
+  unsigned *h_err = (unsigned *)(c->h_out + 14);
+  *h_err = 0;
+  const bool twopass = (n - 1) > 10;
+  if (twopass)
+    HM_CUDA(c, cudaMemcpyAsync(h_err, c->d_ctrl + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+  HM_CUDA(c, cudaStreamSynchronize(c->stream));
+  float ms = 0.f;
+  HM_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  c->last_ms = ms;
+  if (twopass && *h_err)
+    return set_err(c, HM_ERR_TIMEOUT, "two-pass sweep: a dependency wait exceeded its limit; results invalid");
+  out_dd[0] = c->h_out[0];
+  out_dd[1] = c->h_out[1];
+  for (int i = 0; i < q.nq; ++i) {
+    out_dd[2 + 2 * i] = c->h_out[2 * idx[i]];
+    out_dd[3 + 2 * i] = c->h_out[2 * idx[i] + 1];
+  }
+  return HM_OK;
+}
+
+}  // namespace hm

@@ -1,0 +1,163 @@
+/*
+ * hadamag_b200.h -- C ABI of libhadamag_b200.so, the sm_100a (B200) implementation of
+ * HadaMAG.jl's exact stabilizer-Renyi-entropy hot path, its MC_SRE Pauli sampler and
+ * its qutrit Mana phase-space transforms.
+ *
+ * Plain C: pointers and sizes only.  A Julia backend reaches every entry point with
+ * ccall; Python reaches them with ctypes.  Each entry point names the reference
+ * interface it replaces (paths are relative to the HadaMAG.jl repository).
+ *
+ * Conventions
+ *   - Complex arrays are interleaved (re, im) doubles, the memory layout of Julia's
+ *     Vector{ComplexF64} and of numpy complex128.  Device pointers must be 16-byte
+ *     aligned.
+ *   - A state of n qubits has 2^n amplitudes; a state of L qutrits has 3^L.
+ *   - Every call returns HM_OK (0) or a negative HM_ERR_* code; hm_last_error()
+ *     describes the last failure on that context.
+ *   - A context owns one CUDA device, one stream and grow-only device buffers.  Calls
+ *     on one context are serialised by the caller (one context per host thread).
+ *   - Results are returned to host memory; every call synchronises its stream before
+ *     returning unless the name ends in _async.
+ */
+#ifndef HADAMAG_B200_H
+#define HADAMAG_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define HM_ABI_VERSION 1
+
+/* status codes */
+#define HM_OK 0
+#define HM_ERR_ARG -1     /* null pointer, bad enum, bad range                       */
+#define HM_ERR_SIZE -2    /* length not q^n, n outside the supported range           */
+#define HM_ERR_Q -3       /* unsupported Renyi index q                                */
+#define HM_ERR_CUDA -4    /* a CUDA runtime call failed (message in hm_last_error)    */
+#define HM_ERR_OOM -5     /* device allocation failed                                 */
+#define HM_ERR_TIMEOUT -6 /* a bounded device-side wait gave up; results are invalid  */
+#define HM_ERR_ALIGN -7   /* device pointer not 16-byte aligned                      */
+
+/* precision / algorithm selector for the exact-SRE entry points */
+#define HM_FP64 0  /* FP64 butterflies, FP64 double-double reduction            */
+#define HM_FP32 1  /* FP32 butterflies, FP32 per-lane partials, FP64 reduction  */
+#define HM_PLAIN 2 /* the reference CUDA backend's launch structure, FP64       */
+
+typedef struct hm_ctx hm_ctx;
+
+/* Library ABI version (HM_ABI_VERSION). */
+int hm_abi_version(void);
+
+/* Create a context on CUDA device `device`.  Replaces the per-call workspace of
+ * ext/HadaMAGCUDAExt.jl:19-34 (SREChunkWorkspace), which is rebuilt on every SRE call. */
+int hm_create(hm_ctx **ctx, int device);
+
+/* Free every device buffer and the stream of the context. */
+int hm_destroy(hm_ctx *ctx);
+
+/* Text of the last error on this context ("" when none).  Valid until the next call. */
+const char *hm_last_error(hm_ctx *ctx);
+
+/* Run the context's work on an external cudaStream_t (NULL restores the context's own
+ * stream).  Lets a caller time the kernels with events on that stream. */
+int hm_set_stream(hm_ctx *ctx, void *cuda_stream);
+
+/* Device time in milliseconds of the main kernels of the last call (CUDA events on the
+ * context's stream, recorded around the launches that do the transform work). */
+int hm_last_kernel_ms(hm_ctx *ctx, double *ms);
+
+/* ---------------------------------------------------------------------------------- */
+/* Exact SRE                                                                            */
+/* ---------------------------------------------------------------------------------- */
+
+/* Exact stabilizer Renyi entropy over all 4^n Pauli strings.
+ * Replaces SRE(psi, q; backend=:cuda) of ext/HadaMAGCUDAExt.jl:1381-1410 (and the CPU
+ * backends src/Backends/Serial.jl:7-51, src/Backends/Threads.jl:263-314): for each q in
+ * qs[0..nq), out_sre[i] = -log2(m_q / 2^n) with m_q = sum over x, k of (F_x(k)^2)^q, and
+ * out_lost[0] = |1 - p2 / 2^n| with p2 = sum F^2.  As in the reference, for q != 2 the
+ * value is (q-1) times the textbook M_q.
+ * psi: host pointer, 2^n interleaved complex doubles.  1 <= n <= 24 (n <= 21 on the
+ * fused paths; larger n run the HM_PLAIN structure).  1 <= nq <= 4, each q in
+ * [1, 16] (non-integer q allowed). */
+int hm_sre(hm_ctx *ctx, const double *psi, int n, const double *qs, int nq, int precision, double *out_sre,
+           double *out_lost);
+
+/* Same as hm_sre with psi already resident in device memory (16-byte aligned). */
+int hm_sre_dev(hm_ctx *ctx, const double *psi_dev, int n, const double *qs, int nq, int precision,
+               double *out_sre, double *out_lost);
+
+/* Raw sums over the Gray-code indices k in [k_begin, k_end) (X-string x = k ^ (k>>1)),
+ * returned as double-double pairs so that partial ranges combine order-independently:
+ * p2_dd[0] + p2_dd[1] = sum F^2, m_dd[2i] + m_dd[2i+1] = sum (F^2)^{qs[i]}.
+ * Replaces compute_chunk_sre(istart, iend, ...) of src/SRE.jl:338-496 and the per-rank
+ * Gray split of ext/HadaMAGMPICUDAExt.jl:49-56.  psi is a host pointer. */
+int hm_sre_range(hm_ctx *ctx, const double *psi, int n, uint64_t k_begin, uint64_t k_end, const double *qs,
+                 int nq, int precision, double *p2_dd, double *m_dd);
+
+/* Device-pointer variant of hm_sre_range. */
+int hm_sre_range_dev(hm_ctx *ctx, const double *psi_dev, int n, uint64_t k_begin, uint64_t k_end,
+                     const double *qs, int nq, int precision, double *p2_dd, double *m_dd);
+
+/* Batched exact SRE of many states of possibly different qubit counts in one launch
+ * sequence (no reference counterpart; the reference handles one state per call).
+ * psis[s] points to 2^ns[s] interleaved complex doubles (host).  For each state s and
+ * each q: out_sre[s*nq + i]; out_lost[s]. */
+int hm_sre_batched(hm_ctx *ctx, int nstates, const double *const *psis, const int *ns, const double *qs, int nq,
+                   int precision, double *out_sre, double *out_lost);
+
+/* Adjoint (no reference counterpart): value and gradient of SRE_q w.r.t. the real and
+ * imaginary parts of psi.  grad is interleaved: grad[2r] = dSRE/dRe psi_r,
+ * grad[2r+1] = dSRE/dIm psi_r.  The forward transform F_x is recomputed per x, never
+ * stored.  psi host pointer, 1 <= n <= 21, q integer in [1, 8]. */
+int hm_sre_grad(hm_ctx *ctx, const double *psi, int n, double q, double *out_sre, double *grad);
+
+/* ---------------------------------------------------------------------------------- */
+/* MC_SRE                                                                               */
+/* ---------------------------------------------------------------------------------- */
+
+/* Metropolis estimate of SRE_q (replaces MC_SRE of src/Backends/Threads.jl:316-376 with
+ * mc_sre_beta! of src/SRE.jl:110-192).  Chain i runs at beta_i = i / (nbeta - 1).  The
+ * proposal stream is an input: prop_delta[i*nsamples + t] is the XOR of the site bits the
+ * reference draws for step t of chain i (src/SRE.jl:164-170), rs[i*nsamples + t] its
+ * uniform acceptance draw (src/SRE.jl:145).  Outputs: out_m2 = -log2(2^-I + I_add)
+ * (Simpson), per-chain means M2[i], M2ADD[i] = m0/2^n, P2[i]; final_mask[i] (optional,
+ * may be NULL) the chain's current X-string after the last step.  nbeta odd >= 3. */
+int hm_mc_sre(hm_ctx *ctx, const double *psi, int n, double q, int nbeta, int nsamples, const uint64_t *prop_delta,
+              const double *rs, double *out_m2, double *M2, double *M2ADD, double *P2, uint64_t *final_mask);
+
+/* ---------------------------------------------------------------------------------- */
+/* Mana                                                                                 */
+/* ---------------------------------------------------------------------------------- */
+
+/* Mana of a pure L-qutrit state (3^L interleaved complex doubles, host).
+ * Replaces Mana(psi::StateVec{T,3}) of src/Backends/Threads.jl:378-426 with
+ * compute_chunk_mana_qutrits of src/Mana.jl:19-92: log2(sum |W|) / log2(3).  1 <= L <= 12. */
+int hm_mana_pure(hm_ctx *ctx, const double *psi, int L, double *out_mana);
+
+/* Mana of an N-qutrit density matrix (3^N x 3^N, column-major, interleaved complex
+ * doubles, host).  Replaces Mana(rho::DensityMatrix) of src/Mana.jl:305-314:
+ * log2(sum |M^{(x)N} vec9(rho)| / 3^N).  1 <= N <= 8. */
+int hm_mana_mixed(hm_ctx *ctx, const double *rho, int N, double *out_mana);
+
+/* ---------------------------------------------------------------------------------- */
+/* Gray tables (parity checks of the device-side X-string enumeration)                 */
+/* ---------------------------------------------------------------------------------- */
+
+/* Binary Gray table computed on the device, as generate_binary of src/Basis.jl:306-319:
+ * codes[k] = k ^ (k >> 1) (2^n entries), flips[k] = 1-based bit that flips between
+ * codes[k] and codes[k+1] (2^n - 1 entries).  0 <= n <= 30. */
+int hm_gray_table(hm_ctx *ctx, int n, uint64_t *codes, int64_t *flips);
+
+/* q-ary Gray table computed on the device, as generate_general of src/Basis.jl:438-456:
+ * xtab is n x q^n column-major (column k = integer_to_gray(k)), flips has q^n - 1
+ * 1-based digit positions.  2 <= q <= 16, q^n <= 2^26. */
+int hm_gray_table_general(hm_ctx *ctx, int n, int q, int64_t *xtab, int64_t *flips);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HADAMAG_B200_H */

@@ -1,0 +1,856 @@
+/*
+ * hm_oracle.c -- CPU restatement of HadaMAG.jl's exact-SRE / MC_SRE / Mana hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the parity oracle and the timed CPU
+ * baseline.  Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline /
+ * reference arm may load it.  The product (libhadamag_b200.so) never links it.
+ *
+ * Parity status: the Gray-code tables are pinned bit-exactly to the properties the
+ * reference's own tests assert (test/Basis_test.jl:3-25, 70-88).  The reference holds
+ * no golden SRE / Mana values (its tests are backend cross-checks on unseeded states,
+ * test/SRE_test.jl:48-55, test/Mana_test.jl:1-12) and Julia is absent here, so the
+ * numeric functions are pinned only to analytic known answers and to the naive
+ * O(8^n) restatement: "parity unpinned" for SRE/Mana values in the strict sense.
+ *
+ * Every function cites the reference file:line it restates.  All indices follow
+ * the reference's conventions (1-based where the reference is 1-based, noted).
+ *
+ * The fast Walsh-Hadamard transform used by the reference is the external C library
+ * FFHT, pulled as FastHadamardStructuredTransforms_jll v0.0.1 (Project.toml:9,31;
+ * called at src/Helpers.jl:46-55,90).  It is not vendored; or_fwht below is written
+ * from the definition of the in-place unnormalised transform
+ *     v[k] <- sum_r (-1)^{popcount(k&r)} v[r],
+ * applied stage by stage as (a, b) -> (a + b, a - b), the convention the reference's
+ * CUDA extension also uses (ext/HadaMAGCUDAExt.jl:85-90).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#include <omp.h>
+
+#define OR_OK 0
+#define OR_ERR_ARG -1
+
+/* ------------------------------------------------------------------------- */
+/* Gray codes                                                                 */
+/* ------------------------------------------------------------------------- */
+
+/* src/Basis.jl:306-319 (generate_binary): codes[k] = k ^ (k >> 1) for k = 0..2^n-1,
+ * flips[k] (k = 0..2^n-2) = 1-based position of the bit that flips between codes[k]
+ * and codes[k+1]. */
+int or_gray_binary(int n, uint64_t *codes, int64_t *flips) {
+    if (n < 0 || n > 40) return OR_ERR_ARG;
+    uint64_t N = (uint64_t)1 << n;
+    for (uint64_t i = 0; i < N; i++) codes[i] = i ^ (i >> 1);
+    for (uint64_t k = 0; k + 1 < N; k++) flips[k] = (int64_t)__builtin_ctzll(codes[k] ^ codes[k + 1]) + 1;
+    return OR_OK;
+}
+
+/* src/Helpers.jl:18-23 (partition_counts): split n items into P parts, the first
+ * (n mod P) parts one larger; displs are the exclusive prefix sums. */
+void or_partition_counts(int64_t n, int P, int64_t *counts, int64_t *displs) {
+    int64_t base = n / P, rem = n % P, acc = 0;
+    for (int i = 0; i < P; i++) {
+        counts[i] = (i < rem) ? base + 1 : base;
+        displs[i] = acc;
+        acc += counts[i];
+    }
+}
+
+/* src/Basis.jl:76-106 (generate_binary_splitted): the Gray codes of rank's slice of
+ * the partition_counts split and the 1-based flips internal to the slice. */
+int or_gray_binary_split(int n, int rank, int P, uint64_t *codes, int64_t *flips, int64_t *code_off) {
+    if (n < 0 || n > 40 || P < 1 || rank < 0 || rank >= P) return OR_ERR_ARG;
+    int64_t *cnt = malloc(sizeof(int64_t) * P), *dsp = malloc(sizeof(int64_t) * P);
+    or_partition_counts((int64_t)1 << n, P, cnt, dsp);
+    int64_t off = dsp[rank], c = cnt[rank];
+    for (int64_t j = 0; j < c; j++) {
+        uint64_t i = (uint64_t)(off + j);
+        codes[j] = i ^ (i >> 1);
+    }
+    for (int64_t j = 0; j + 1 < c; j++) flips[j] = (int64_t)__builtin_ctzll(codes[j] ^ codes[j + 1]) + 1;
+    *code_off = off;
+    free(cnt);
+    free(dsp);
+    return OR_OK;
+}
+
+/* src/Basis.jl:415-425 (integer_to_gray): base-q digits of val least-significant
+ * first, padded to n, folded from the most significant digit down with a running
+ * shift: gray[i] = (digit[i] + shift) mod q; shift += q - gray[i]. */
+static void integer_to_gray(int64_t val, int q, int n, int64_t *gray) {
+    int64_t digit[64];
+    for (int i = 0; i < n; i++) {
+        digit[i] = val % q;
+        val /= q;
+    }
+    int64_t shift = 0;
+    for (int i = n - 1; i >= 0; i--) {
+        gray[i] = (digit[i] + shift) % q;
+        shift += q - gray[i];
+    }
+}
+
+/* src/Basis.jl:438-456 (generate_general): XTAB is n x q^n, column-major (column k is
+ * integer_to_gray(k)), flips[k] = 1-based first digit where columns k and k+1 differ. */
+int or_gray_general(int n, int q, int64_t *xtab, int64_t *flips) {
+    if (n < 0 || n > 40 || q < 2) return OR_ERR_ARG;
+    int64_t N = 1;
+    for (int i = 0; i < n; i++) N *= q;
+    for (int64_t k = 0; k < N; k++) integer_to_gray(k, q, n, xtab + k * n);
+    for (int64_t k = 0; k + 1 < N; k++) {
+        int64_t pos = 0;
+        for (int i = 0; i < n; i++)
+            if (xtab[k * n + i] != xtab[(k + 1) * n + i]) {
+                pos = i + 1;
+                break;
+            }
+        flips[k] = pos;
+    }
+    return OR_OK;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Walsh-Hadamard transform (from the definition; see header)                 */
+/* ------------------------------------------------------------------------- */
+
+static void fwht_block(double *restrict p, int B) {
+    const int64_t bs = (int64_t)1 << B;
+    /* stages 0..2 as radix-8 on consecutive elements */
+    int s0 = 0;
+    if (B >= 3) {
+        for (int64_t i = 0; i < bs; i += 8) {
+            double a0 = p[i], a1 = p[i + 1], a2 = p[i + 2], a3 = p[i + 3];
+            double a4 = p[i + 4], a5 = p[i + 5], a6 = p[i + 6], a7 = p[i + 7];
+            double b0 = a0 + a1, b1 = a0 - a1, b2 = a2 + a3, b3 = a2 - a3;
+            double b4 = a4 + a5, b5 = a4 - a5, b6 = a6 + a7, b7 = a6 - a7;
+            double c0 = b0 + b2, c2 = b0 - b2, c1 = b1 + b3, c3 = b1 - b3;
+            double c4 = b4 + b6, c6 = b4 - b6, c5 = b5 + b7, c7 = b5 - b7;
+            p[i] = c0 + c4; p[i + 4] = c0 - c4;
+            p[i + 1] = c1 + c5; p[i + 5] = c1 - c5;
+            p[i + 2] = c2 + c6; p[i + 6] = c2 - c6;
+            p[i + 3] = c3 + c7; p[i + 7] = c3 - c7;
+        }
+        s0 = 3;
+    }
+    for (int s = s0; s < B; s++) {
+        const int64_t h = (int64_t)1 << s;
+        for (int64_t i = 0; i < bs; i += 2 * h)
+            for (int64_t j = i; j < i + h; j++) {
+                double a = p[j], b = p[j + h];
+                p[j] = a + b;
+                p[j + h] = a - b;
+            }
+    }
+}
+
+/* in-place unnormalised WHT of v[0 .. 2^L) */
+void or_fwht(double *restrict v, int L) {
+    if (L <= 0) return;
+    const int64_t N = (int64_t)1 << L;
+    const int B = L < 11 ? L : 11; /* 16 KiB blocks stay in L1 */
+    const int64_t bs = (int64_t)1 << B;
+    for (int64_t base = 0; base < N; base += bs) fwht_block(v + base, B);
+    int s = B;
+    /* remaining stages two at a time (radix-4) */
+    for (; s + 1 < L; s += 2) {
+        const int64_t h = (int64_t)1 << s;
+        for (int64_t i = 0; i < N; i += 4 * h)
+            for (int64_t j = i; j < i + h; j++) {
+                double a = v[j], b = v[j + h], c = v[j + 2 * h], d = v[j + 3 * h];
+                double ab = a + b, amb = a - b, cd = c + d, cmd = c - d;
+                v[j] = ab + cd;
+                v[j + 2 * h] = ab - cd;
+                v[j + h] = amb + cmd;
+                v[j + 3 * h] = amb - cmd;
+            }
+    }
+    for (; s < L; s++) {
+        const int64_t h = (int64_t)1 << s;
+        for (int64_t i = 0; i < N; i += 2 * h)
+            for (int64_t j = i; j < i + h; j++) {
+                double a = v[j], b = v[j + h];
+                v[j] = a + b;
+                v[j + h] = a - b;
+            }
+    }
+}
+
+/* ------------------------------------------------------------------------- */
+/* Exact SRE                                                                  */
+/* ------------------------------------------------------------------------- */
+
+/* (F^2)^q for the reference's two cases: q == 2 -> p*p (src/SRE.jl:239), other q ->
+ * p^q (src/SRE.jl:262; integer q by repeated product, non-integer by pow). */
+static inline double pow_q(double p, double q) {
+    if (q == 2.0) return p * p;
+    if (q == floor(q) && q >= 1.0 && q <= 16.0) {
+        double r = p;
+        for (int i = 1; i < (int)q; i++) r *= p;
+        return r;
+    }
+    return pow(p, q);
+}
+
+/* src/SRE.jl:225-278 (kahan_accumulate): per-x compensated sums of p = v^2 and of
+ * (p)^q over the transformed vector. */
+static void kahan_accumulate(const double *restrict v, int64_t dim, double q, double *p2_out, double *m_out) {
+    double p2_sum = 0.0, p2_c = 0.0, m_sum = 0.0, m_c = 0.0;
+    for (int64_t i = 0; i < dim; i++) {
+        double p = v[i] * v[i];
+        double pq = pow_q(p, q);
+        double y = p - p2_c;
+        double t = p2_sum + y;
+        p2_c = (t - p2_sum) - y;
+        p2_sum = t;
+        double y2 = pq - m_c;
+        double t2 = m_sum + y2;
+        m_c = (t2 - m_sum) - y2;
+        m_sum = t2;
+    }
+    *p2_out = p2_sum;
+    *m_out = m_sum;
+}
+
+/* src/SRE.jl:509-540 (flip_and_update_mask!): inVR[r] = X1[r]*TMP1[r^mask] +
+ * X2[r]*TMP2[r^mask] with mask = old mask ^ (1 << site); written as the reference's
+ * muladd(X1, TMP1[j], X2 * TMP2[j]).  Returns the new mask. */
+static uint64_t flip_and_update_mask(int site, int64_t dim, uint64_t mask, const double *TMP1, const double *TMP2,
+                                     const double *X1, const double *X2, double *inVR) {
+    uint64_t newmask = mask ^ ((uint64_t)1 << site);
+    for (int64_t r = 0; r < dim; r++) {
+        uint64_t j = (uint64_t)r ^ newmask;
+        inVR[r] = fma(X1[r], TMP1[j], X2[r] * TMP2[j]);
+    }
+    return newmask;
+}
+
+typedef struct {
+    int n;
+    int64_t dim;
+    double *X1, *X2, *TMP1, *TMP2; /* src/Backends/Threads.jl:270-283 */
+} sre_prep;
+
+static int sre_prep_init(sre_prep *s, const double *psi, int n) {
+    s->n = n;
+    s->dim = (int64_t)1 << n;
+    size_t bytes = sizeof(double) * (size_t)s->dim;
+    s->X1 = malloc(bytes);
+    s->X2 = malloc(bytes);
+    s->TMP1 = malloc(bytes);
+    s->TMP2 = malloc(bytes);
+    if (!s->X1 || !s->X2 || !s->TMP1 || !s->TMP2) return OR_ERR_ARG;
+    for (int64_t i = 0; i < s->dim; i++) {
+        double r = psi[2 * i], im = psi[2 * i + 1];
+        s->X1[i] = r;
+        s->X2[i] = im;
+        s->TMP1[i] = r + im;
+        s->TMP2[i] = im - r;
+    }
+    return OR_OK;
+}
+
+static void sre_prep_free(sre_prep *s) {
+    free(s->X1);
+    free(s->X2);
+    free(s->TMP1);
+    free(s->TMP2);
+}
+
+/* src/SRE.jl:338-411 and 424-496 (compute_chunk_sre): Gray walk over 1-based Gray
+ * indices ix = istart..iend.  At the chunk head the mask is rebuilt from all set bits of
+ * XTAB[istart] (or one plain blend when it is 0); afterwards one site flips per step.
+ * Per x: blend, FWHT, Kahan sums; the chunk totals p2SAM, mSAM are plain sums. */
+static void sre_chunk(const sre_prep *s, double q, int64_t istart, int64_t iend, double *inVR, double *p2_out,
+                      double *m_out) {
+    const int64_t dim = s->dim;
+    double p2SAM = 0.0, mSAM = 0.0;
+    uint64_t mask = 0;
+    for (int64_t ix = istart; ix <= iend; ix++) {
+        if (ix == istart) {
+            uint64_t k = (uint64_t)(ix - 1);
+            uint64_t bits = k ^ (k >> 1); /* XTAB[ix] */
+            if (bits == 0) {
+                for (int64_t r = 0; r < dim; r++) inVR[r] = fma(s->X1[r], s->TMP1[r], s->X2[r] * s->TMP2[r]);
+            } else {
+                uint64_t m = bits;
+                while (m != 0) {
+                    int site = __builtin_ctzll(m);
+                    mask = flip_and_update_mask(site, dim, mask, s->TMP1, s->TMP2, s->X1, s->X2, inVR);
+                    m &= m - 1;
+                }
+            }
+        } else {
+            /* Zwhere[ix-1] - 1: 0-based site flipping between XTAB[ix-1] and XTAB[ix] */
+            uint64_t a = (uint64_t)(ix - 2), b = (uint64_t)(ix - 1);
+            int site = __builtin_ctzll((a ^ (a >> 1)) ^ (b ^ (b >> 1)));
+            mask = flip_and_update_mask(site, dim, mask, s->TMP1, s->TMP2, s->X1, s->X2, inVR);
+        }
+        or_fwht(inVR, s->n);
+        double lp2, lm;
+        kahan_accumulate(inVR, dim, q, &lp2, &lm);
+        p2SAM += lp2;
+        mSAM += lm;
+    }
+    *p2_out = p2SAM;
+    *m_out = mSAM;
+}
+
+/* Raw sums (p2SAM, mSAM) over 1-based Gray indices [istart, iend] split over nthreads
+ * exactly as src/Backends/Threads.jl:192-257 (threaded_chunk_reduce): static contiguous
+ * partition_counts slices, per-thread compute_chunk_sre, per-thread results summed in
+ * thread order. */
+int or_sre_sums(const double *psi, int n, double q, int64_t istart, int64_t iend, int nthreads, double *p2_out,
+                double *m_out) {
+    if (n < 0 || n > 30 || nthreads < 1) return OR_ERR_ARG;
+    const int64_t dim = (int64_t)1 << n;
+    if (istart < 1 || iend > dim || iend < istart - 1) return OR_ERR_ARG;
+    sre_prep s;
+    if (sre_prep_init(&s, psi, n) != OR_OK) return OR_ERR_ARG;
+    const int64_t len = iend - istart + 1;
+    int64_t *tcnt = malloc(sizeof(int64_t) * nthreads), *tdisp = malloc(sizeof(int64_t) * nthreads);
+    double *acc = calloc(2 * (size_t)nthreads, sizeof(double));
+    or_partition_counts(len, nthreads, tcnt, tdisp);
+#pragma omp parallel num_threads(nthreads)
+    {
+        int tid = omp_get_thread_num();
+        if (tid < nthreads && tcnt[tid] > 0) {
+            double *inVR = malloc(sizeof(double) * (size_t)dim);
+            int64_t a = istart + tdisp[tid], b = istart + tdisp[tid] + tcnt[tid] - 1;
+            sre_chunk(&s, q, a, b, inVR, &acc[2 * tid], &acc[2 * tid + 1]);
+            free(inVR);
+        }
+    }
+    double p2 = 0.0, m = 0.0;
+    for (int t = 0; t < nthreads; t++) {
+        p2 += acc[2 * t];
+        m += acc[2 * t + 1];
+    }
+    *p2_out = p2;
+    *m_out = m;
+    free(tcnt);
+    free(tdisp);
+    free(acc);
+    sre_prep_free(&s);
+    return OR_OK;
+}
+
+/* src/Backends/Threads.jl:263-314 (SRE): (-log2(m/dim), |1 - p2/dim|) over all 2^n
+ * X-strings.  With nthreads == 1 this is src/Backends/Serial.jl:7-51. */
+int or_sre(const double *psi, int n, double q, int nthreads, double *sre, double *lost) {
+    double p2, m;
+    const int64_t dim = (int64_t)1 << n;
+    int rc = or_sre_sums(psi, n, q, 1, dim, nthreads, &p2, &m);
+    if (rc != OR_OK) return rc;
+    *sre = -log2(m / (double)dim);
+    *lost = fabs(1.0 - p2 / (double)dim);
+    return OR_OK;
+}
+
+/* src/SRE.jl:601-679 (iphase, expval_pauli_mask): <psi|P_{x,z}|psi> =
+ * real(i^{|x&z|} * sum_b (-1)^{b.z} conj(psi[b^x]) psi[b]). */
+static double expval_pauli_mask(const double *psi, int64_t N, uint64_t x, uint64_t z) {
+    int k = __builtin_popcountll(x & z) & 3;
+    double sr = 0.0, si = 0.0;
+    for (int64_t b = 0; b < N; b++) {
+        uint64_t bp = (uint64_t)b ^ x;
+        double sign = (__builtin_popcountll((uint64_t)b & z) & 1) ? -1.0 : 1.0;
+        double ar = psi[2 * bp], ai = -psi[2 * bp + 1]; /* conj(psi[b^x]) */
+        double br = psi[2 * b], bi = psi[2 * b + 1];
+        sr += sign * (ar * br - ai * bi);
+        si += sign * (ar * bi + ai * br);
+    }
+    /* real(i^k * (sr + i si)) */
+    switch (k) {
+        case 0: return sr;
+        case 1: return -si;
+        case 2: return -sr;
+        default: return si;
+    }
+}
+
+/* src/SRE.jl:690-749 (naive_SRE): -log2( sum over all 4^n Pauli strings of
+ * (e^2)^q / N ) with per-thread compensated sums, the Pauli string decoded from the
+ * base-4 digits of idx (0 -> I, 1 -> X, 2 -> Y, 3 -> Z). */
+int or_naive_sre(const double *psi, int n, int q, int nthreads, double *out) {
+    if (n < 0 || n > 14 || q < 1 || nthreads < 1) return OR_ERR_ARG;
+    const int64_t N = (int64_t)1 << n;
+    const int64_t total = (int64_t)1 << (2 * n);
+    double *partial = calloc((size_t)nthreads, sizeof(double));
+    double *cval = calloc((size_t)nthreads, sizeof(double));
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int64_t idx = 0; idx < total; idx++) {
+        int tid = omp_get_thread_num();
+        uint64_t tmp = (uint64_t)idx, x = 0, z = 0;
+        for (int j = 0; j < n; j++) {
+            uint64_t d = tmp & 3;
+            if (d == 1) x |= (uint64_t)1 << j;
+            else if (d == 2) { x |= (uint64_t)1 << j; z |= (uint64_t)1 << j; }
+            else if (d == 3) z |= (uint64_t)1 << j;
+            tmp >>= 2;
+        }
+        double e = expval_pauli_mask(psi, N, x, z);
+        double p = e * e, pq = p;
+        for (int i = 1; i < q; i++) pq *= p;
+        double y = pq - cval[tid];
+        double t = partial[tid] + y;
+        cval[tid] = (t - partial[tid]) - y;
+        partial[tid] = t;
+    }
+    double s = 0.0;
+    for (int t = 0; t < nthreads; t++) s += partial[t];
+    *out = -log2(s / (double)N);
+    free(partial);
+    free(cval);
+    return OR_OK;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Monte-Carlo SRE (Metropolis over X-strings)                                */
+/* ------------------------------------------------------------------------- */
+
+/* src/SRE.jl:195-223 (compute_moments): plain sums of v^2 and of (v^2)^q. */
+static void compute_moments(const double *v, int64_t dim, double q, double *s2, double *s4) {
+    double a = 0.0, b = 0.0;
+    for (int64_t i = 0; i < dim; i++) {
+        double y2 = v[i] * v[i];
+        a += y2;
+        if (q == 2.0) b = fma(y2, y2, b);
+        else b += pow_q(y2, q);
+    }
+    *s2 = a;
+    *s4 = b;
+}
+
+/* src/SRE.jl:127-140 (blend_mask!, sample_mask!): inVR[i] = muladd(re X[i],
+ * tmp1[i^mask], im X[i] * tmp2[i^mask]), FWHT, moments; returns (p2/dim, m_q). */
+static void sample_mask(const sre_prep *s, double q, uint64_t mask, double *inVR, double *p2, double *mq) {
+    for (int64_t i = 0; i < s->dim; i++) {
+        uint64_t j = (uint64_t)i ^ mask;
+        inVR[i] = fma(s->X1[i], s->TMP1[j], s->X2[i] * s->TMP2[j]);
+    }
+    or_fwht(inVR, s->n);
+    double a, b;
+    compute_moments(inVR, s->dim, q, &a, &b);
+    *p2 = a / (double)s->dim;
+    *mq = b;
+}
+
+/* src/SRE.jl:110-192 (mc_sre_beta!) with the proposal stream injected: the reference
+ * draws tries[t] = floor(9 u) + 1 site flips, each site = rand(rng, 1:L), and
+ * propDelta[t] = XOR of those site bits, plus rs[t] uniform in [0,1)
+ * (src/SRE.jl:142-145,164-170).  Those draws are inputs here (prop_delta, rs).
+ * out5 = (mean M2, mean M2^2, m0/dim, mean P2, n); accepted (optional, nsamples)
+ * records the current mask after each step. */
+int or_mc_sre_beta(const double *psi, int n, double q, int nsamples, double beta, const uint64_t *prop_delta,
+                   const double *rs, double *out5, uint64_t *masks_out) {
+    if (n < 0 || n > 30 || nsamples < 1) return OR_ERR_ARG;
+    sre_prep s;
+    if (sre_prep_init(&s, psi, n) != OR_OK) return OR_ERR_ARG;
+    double *inVR = malloc(sizeof(double) * (size_t)s.dim);
+    double p2_0, m0;
+    sample_mask(&s, q, 0, inVR, &p2_0, &m0);
+    uint64_t currMask = 0;
+    double currPROB = 1e-120, currM2 = 0.0, currP2 = p2_0;
+    double sM2 = 0.0, sM2sq = 0.0, sP2 = 0.0;
+    int64_t cnt = 0;
+    for (int t = 0; t < nsamples; t++) {
+        uint64_t propMask = currMask ^ prop_delta[t];
+        double p2_prop, m_prop;
+        sample_mask(&s, q, propMask, inVR, &p2_prop, &m_prop);
+        double pb = pow(m_prop, beta);
+        double r = rs[t];
+        if ((r < pb / currPROB) && (propMask != 0)) {
+            currMask = propMask;
+            currPROB = pb;
+            currM2 = -log2(m_prop);
+            currP2 = p2_prop;
+        }
+        sM2 += currM2;
+        sM2sq += currM2 * currM2;
+        sP2 += currP2;
+        cnt += 1;
+        if (masks_out) masks_out[t] = currMask;
+    }
+    out5[0] = sM2 / (double)cnt;
+    out5[1] = sM2sq / (double)cnt;
+    out5[2] = m0 / (double)s.dim;
+    out5[3] = sP2 / (double)cnt;
+    out5[4] = (double)cnt;
+    free(inVR);
+    sre_prep_free(&s);
+    return OR_OK;
+}
+
+/* src/Helpers.jl:223-236 (integrate_simpson_uniform). */
+double or_simpson_uniform(const double *x, const double *y, int npts) {
+    int n = npts - 1;
+    if (n <= 0 || n % 2 != 0) return NAN;
+    double h = (x[npts - 1] - x[0]) / n;
+    double odd = 0.0, even = 0.0;
+    for (int i = 1; i < npts - 1; i += 2) odd += y[i];
+    for (int i = 2; i < npts - 1; i += 2) even += y[i];
+    return (h / 3.0) * (y[0] + y[npts - 1] + 4.0 * odd + 2.0 * even);
+}
+
+/* src/Backends/Threads.jl:316-376 (MC_SRE): one chain per beta_i = (i-1)/(Nbeta-1),
+ * Simpson over M2 and M2ADD, m2 = -log2(2^-I + I_add).  prop_delta and rs hold
+ * Nbeta consecutive streams of nsamples each. */
+int or_mc_sre(const double *psi, int n, double q, int nbeta, int nsamples, const uint64_t *prop_delta,
+              const double *rs, int nthreads, double *m2_out, double *M2, double *M2ADD, double *P2) {
+    if (nbeta < 3 || nbeta % 2 != 1) return OR_ERR_ARG;
+    int rc = OR_OK;
+#pragma omp parallel for num_threads(nthreads) schedule(static)
+    for (int i = 0; i < nbeta; i++) {
+        double beta = (double)i / (double)(nbeta - 1);
+        double o[5];
+        int r = or_mc_sre_beta(psi, n, q, nsamples, beta, prop_delta + (size_t)i * nsamples,
+                               rs + (size_t)i * nsamples, o, NULL);
+        if (r != OR_OK) rc = r;
+        M2[i] = o[0];
+        M2ADD[i] = o[2];
+        P2[i] = o[3];
+    }
+    if (rc != OR_OK) return rc;
+    double *x = malloc(sizeof(double) * nbeta);
+    for (int i = 0; i < nbeta; i++) x[i] = (double)i / (double)(nbeta - 1);
+    double I_res = or_simpson_uniform(x, M2, nbeta);
+    double I_add = or_simpson_uniform(x, M2ADD, nbeta);
+    *m2_out = -log2(pow(2.0, -I_res) + I_add);
+    free(x);
+    return OR_OK;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Mana (qutrits)                                                             */
+/* ------------------------------------------------------------------------- */
+
+/* src/Helpers.jl:246-292 (fast_hadamard_qutrit!): L stages of the 3-point DFT
+ * (a, b, c) -> (a+b+c, a+w b+w^2 c, a+w^2 b+w c), w = e^{2 pi i/3}, on interleaved
+ * complex data of length N = 3^L. */
+void or_fht_qutrit(double *v, int64_t N) {
+    const double wr = -0.5, wi = sqrt(3.0) / 2.0;
+    int64_t step = 1;
+    while (step < N) {
+        int64_t jump = 3 * step;
+        for (int64_t i = 0; i < N; i += jump)
+            for (int64_t j = 0; j < step; j++) {
+                int64_t ia = i + j, ib = ia + step, ic = ia + 2 * step;
+                double ar = v[2 * ia], ai = v[2 * ia + 1];
+                double br = v[2 * ib], bi = v[2 * ib + 1];
+                double cr = v[2 * ic], ci = v[2 * ic + 1];
+                double r0 = ar + br + cr, i0 = ai + bi + ci;
+                double r1 = ar + wr * (br + cr) - wi * (bi - ci);
+                double i1 = ai + wr * (bi + ci) + wi * (br - cr);
+                double r2 = ar + wr * (br + cr) + wi * (bi - ci);
+                double i2 = ai + wr * (bi + ci) - wi * (br - cr);
+                v[2 * ia] = r0; v[2 * ia + 1] = i0;
+                v[2 * ib] = r1; v[2 * ib + 1] = i1;
+                v[2 * ic] = r2; v[2 * ic + 1] = i2;
+            }
+        step = jump;
+    }
+}
+
+/* src/Mana.jl:97-113 (rotate_perm_site!): cyclic update of the permutation for the
+ * qutrit shift at 1-based site, k = 1 (0->1->2) or k = 2 (0->2->1). */
+static void rotate_perm_site(int64_t *perm, int64_t len, int site, int k) {
+    int64_t stride = 1;
+    for (int i = 1; i < site; i++) stride *= 3;
+    int64_t block = 3 * stride;
+    for (int64_t bs = 0; bs < len; bs += block)
+        for (int64_t off = 0; off < stride; off++) {
+            int64_t i0 = bs + off, i1 = i0 + stride, i2 = i1 + stride;
+            int64_t p0 = perm[i0], p1 = perm[i1], p2 = perm[i2];
+            if (k == 1) { perm[i0] = p1; perm[i1] = p2; perm[i2] = p0; }
+            else { perm[i0] = p2; perm[i1] = p0; perm[i2] = p1; }
+        }
+}
+
+/* src/Mana.jl:19-92 (compute_chunk_mana_qutrits): columns ix = istart..iend (1-based)
+ * of the ternary Gray table; per column inV[r] = conj(psi[perm[r]]) * (psi[perm[AA[r]]]
+ * / 3^L), qutrit Hadamard, running Kahan sum of |inV| across the chunk; the
+ * permutation advances by one single-site rotation per column. */
+static double mana_chunk(const double *psi, int L, int64_t dim, const int64_t *XTAB, const int64_t *Zwhere,
+                         const int64_t *AA, int64_t istart, int64_t iend, double *inV) {
+    const double invdim = 1.0 / (double)dim;
+    int64_t *perm = malloc(sizeof(int64_t) * (size_t)dim);
+    for (int64_t i = 0; i < dim; i++) perm[i] = i;
+    for (int s = 1; s <= L; s++) {
+        int64_t k = XTAB[(istart - 1) * L + (s - 1)] % 3;
+        if (k == 1) rotate_perm_site(perm, dim, s, 1);
+        else if (k == 2) rotate_perm_site(perm, dim, s, 2);
+    }
+    double p2SAM = 0.0, c = 0.0;
+    for (int64_t ix = istart; ix <= iend; ix++) {
+        for (int64_t r = 0; r < dim; r++) {
+            int64_t pa = perm[r], pb = perm[AA[r]];
+            double ar = psi[2 * pa], ai = psi[2 * pa + 1];
+            double br = psi[2 * pb] * invdim, bi = psi[2 * pb + 1] * invdim;
+            /* conj(a) * b */
+            inV[2 * r] = ar * br + ai * bi;
+            inV[2 * r + 1] = ar * bi - ai * br;
+        }
+        or_fht_qutrit(inV, dim);
+        for (int64_t i = 0; i < dim; i++) {
+            double ap = hypot(inV[2 * i], inV[2 * i + 1]);
+            double y = ap - c;
+            double t = p2SAM + y;
+            c = (t - p2SAM) - y;
+            p2SAM = t;
+        }
+        if (ix < iend) {
+            int s = (int)Zwhere[ix - 1];
+            int64_t kstep = ((XTAB[ix * L + (s - 1)] - XTAB[(ix - 1) * L + (s - 1)]) % 3 + 3) % 3;
+            rotate_perm_site(perm, dim, s, (int)kstep);
+        }
+    }
+    free(perm);
+    return p2SAM;
+}
+
+/* Sum of |W| over the 1-based ternary Gray columns [istart, iend], threaded as
+ * src/Backends/Threads.jl:378-426 (static partition, thread-ordered sum). */
+int or_mana_sum(const double *psi, int L, int64_t istart, int64_t iend, int nthreads, double *sum_out) {
+    if (L < 0 || L > 16 || nthreads < 1) return OR_ERR_ARG;
+    int64_t dim = 1;
+    for (int i = 0; i < L; i++) dim *= 3;
+    if (istart < 1 || iend > dim || iend < istart) return OR_ERR_ARG;
+    int64_t *XTAB = malloc(sizeof(int64_t) * (size_t)dim * (L > 0 ? L : 1));
+    int64_t *Zwhere = malloc(sizeof(int64_t) * (size_t)dim);
+    or_gray_general(L, 3, XTAB, Zwhere);
+    /* src/Backends/Threads.jl:384-397: AA = digitwise negation mod 3 (0-based here) */
+    int64_t *AA = malloc(sizeof(int64_t) * (size_t)dim);
+    for (int64_t i = 0; i < dim; i++) {
+        int64_t x = i, y = 0, pw = 1;
+        for (int k = 0; k < L; k++) {
+            int64_t d = x % 3;
+            x /= 3;
+            y += ((3 - d) % 3) * pw;
+            pw *= 3;
+        }
+        AA[i] = y;
+    }
+    const int64_t len = iend - istart + 1;
+    int64_t *tcnt = malloc(sizeof(int64_t) * nthreads), *tdisp = malloc(sizeof(int64_t) * nthreads);
+    double *acc = calloc((size_t)nthreads, sizeof(double));
+    or_partition_counts(len, nthreads, tcnt, tdisp);
+#pragma omp parallel num_threads(nthreads)
+    {
+        int tid = omp_get_thread_num();
+        if (tcnt[tid] > 0) {
+            double *inV = malloc(sizeof(double) * 2 * (size_t)dim);
+            acc[tid] = mana_chunk(psi, L, dim, XTAB, Zwhere, AA, istart + tdisp[tid],
+                                  istart + tdisp[tid] + tcnt[tid] - 1, inV);
+            free(inV);
+        }
+    }
+    double s = 0.0;
+    for (int t = 0; t < nthreads; t++) s += acc[t];
+    *sum_out = s;
+    free(XTAB);
+    free(Zwhere);
+    free(AA);
+    free(tcnt);
+    free(tdisp);
+    free(acc);
+    return OR_OK;
+}
+
+/* src/Backends/Threads.jl:378-426 (Mana): log2(S)/log2(3). */
+int or_mana_pure(const double *psi, int L, int nthreads, double *mana) {
+    int64_t dim = 1;
+    for (int i = 0; i < L; i++) dim *= 3;
+    double s;
+    int rc = or_mana_sum(psi, L, 1, dim, nthreads, &s);
+    if (rc != OR_OK) return rc;
+    *mana = log2(s) / log2(3.0);
+    return OR_OK;
+}
+
+/* complex helpers (interleaved) */
+typedef struct { double re, im; } cplx;
+static inline cplx cmul(cplx a, cplx b) { cplx r = {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; return r; }
+static inline cplx cadd(cplx a, cplx b) { cplx r = {a.re + b.re, a.im + b.im}; return r; }
+static inline cplx cconj(cplx a) { cplx r = {a.re, -a.im}; return r; }
+
+static void mat3_mul(const cplx *A, const cplx *B, cplx *C) { /* row-major 3x3 */
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) {
+            cplx s = {0, 0};
+            for (int k = 0; k < 3; k++) s = cadd(s, cmul(A[3 * i + k], B[3 * k + j]));
+            C[3 * i + j] = s;
+        }
+}
+
+/* src/Mana.jl:123-182 (build_single_qutrit_M): M is 9x9, row idx = vec_colmajor(A_u^T),
+ * A_u = T_u A0 T_u^dagger, T_{a,a'} = w^{(-2 a a') mod 3} Z^a X^{a'}, idx = 3a + a',
+ * A0 = (1/3) sum_u T_u.  Output M row-major: M[9*idx + c]. */
+void or_single_qutrit_M(double *Mout) {
+    const double PI = 3.14159265358979323846;
+    cplx w = {cos(2 * PI / 3), sin(2 * PI / 3)};
+    cplx X[9] = {{0}}, Z[9] = {{0}}, I3[9] = {{0}};
+    for (int k = 0; k < 3; k++) {
+        X[3 * ((k + 1) % 3) + k].re = 1.0; /* X[(k+1)%3, k] = 1 */
+        I3[3 * k + k].re = 1.0;
+    }
+    cplx wp[3] = {{1, 0}, w, cmul(w, w)};
+    for (int k = 0; k < 3; k++) Z[3 * k + k] = wp[k]; /* w^k */
+    cplx Zp[3][9], Xp[3][9];
+    memcpy(Zp[0], I3, sizeof(I3));
+    memcpy(Zp[1], Z, sizeof(Z));
+    mat3_mul(Z, Z, Zp[2]);
+    memcpy(Xp[0], I3, sizeof(I3));
+    memcpy(Xp[1], X, sizeof(X));
+    mat3_mul(X, X, Xp[2]);
+    cplx T[9][9];
+    for (int a = 0; a < 3; a++)
+        for (int ap = 0; ap < 3; ap++) {
+            int idx = 3 * a + ap;
+            int e = ((-2 * a * ap) % 3 + 3) % 3;
+            /* w^e computed as a power of w, like the reference's w^exponent */
+            cplx ph = {1, 0};
+            for (int i = 0; i < e; i++) ph = cmul(ph, w);
+            cplx ZX[9];
+            mat3_mul(Zp[a], Xp[ap], ZX);
+            for (int i = 0; i < 9; i++) T[idx][i] = cmul(ph, ZX[i]);
+        }
+    cplx A0[9] = {{0}};
+    for (int u = 0; u < 9; u++)
+        for (int i = 0; i < 9; i++) A0[i] = cadd(A0[i], T[u][i]);
+    for (int i = 0; i < 9; i++) { A0[i].re /= 3.0; A0[i].im /= 3.0; }
+    for (int idx = 0; idx < 9; idx++) {
+        cplx Td[9], tmp[9], Au[9];
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) Td[3 * i + j] = cconj(T[idx][3 * j + i]);
+        mat3_mul(T[idx], A0, tmp);
+        mat3_mul(tmp, Td, Au);
+        /* vec(transpose(Au)) column-major: c = i + 3 j holds Au^T[i, j] = Au[j, i] */
+        for (int i = 0; i < 3; i++)
+            for (int j = 0; j < 3; j++) {
+                int c = i + 3 * j;
+                Mout[2 * (9 * idx + c)] = Au[3 * j + i].re;
+                Mout[2 * (9 * idx + c) + 1] = Au[3 * j + i].im;
+            }
+    }
+}
+
+/* src/Mana.jl:190-228 (vec_rho_tensor_N) + 236-281 (apply_M_tensor_N_inplace!) +
+ * 305-314 (Mana(rho)): v[p] = rho[r0, c0] with p's base-9 digit for site k (site 1 most
+ * significant) = 3 i_k + j_k, i_k / j_k the k-th most significant ternary digits of r0 /
+ * c0; w = M^{(x)N} v leg by leg (leg 1 = most significant digit); mana = log2(sum|w| /
+ * 3^N).  rho is column-major interleaved complex: rho[r0 + dim*c0]. */
+int or_mana_mixed(const double *rho, int N, double *mana_out, double *w_out) {
+    if (N < 0 || N > 8) return OR_ERR_ARG;
+    int64_t dim = 1, op = 1;
+    for (int i = 0; i < N; i++) { dim *= 3; op *= 9; }
+    double Mre[162];
+    or_single_qutrit_M(Mre);
+    cplx M[81];
+    for (int i = 0; i < 81; i++) { M[i].re = Mre[2 * i]; M[i].im = Mre[2 * i + 1]; }
+    cplx *v = calloc((size_t)op, sizeof(cplx));
+    int idig[16], jdig[16];
+    for (int64_t c0 = 0; c0 < dim; c0++) {
+        int64_t t = c0;
+        for (int k = N - 1; k >= 0; k--) { jdig[k] = (int)(t % 3); t /= 3; }
+        for (int64_t r0 = 0; r0 < dim; r0++) {
+            int64_t u = r0;
+            for (int k = N - 1; k >= 0; k--) { idig[k] = (int)(u % 3); u /= 3; }
+            int64_t p = 0;
+            for (int k = 0; k < N; k++) p = p * 9 + (3 * idig[k] + jdig[k]);
+            v[p].re = rho[2 * (r0 + dim * c0)];
+            v[p].im = rho[2 * (r0 + dim * c0) + 1];
+        }
+    }
+    cplx x[9], y[9];
+    for (int leg = 1; leg <= N; leg++) {
+        int64_t stride = 1;
+        for (int i = 0; i < N - leg; i++) stride *= 9;
+        int64_t block = stride * 9, nblocks = op / block;
+        for (int64_t b = 0; b < nblocks; b++)
+            for (int64_t ofs = 0; ofs < stride; ofs++) {
+                int64_t base = b * block + ofs;
+                for (int a = 0; a < 9; a++) x[a] = v[base + a * stride];
+                for (int r = 0; r < 9; r++) {
+                    cplx s = {0, 0};
+                    for (int c = 0; c < 9; c++) s = cadd(s, cmul(M[9 * r + c], x[c]));
+                    y[r] = s;
+                }
+                for (int a = 0; a < 9; a++) v[base + a * stride] = y[a];
+            }
+    }
+    double s = 0.0;
+    for (int64_t i = 0; i < op; i++) s += hypot(v[i].re, v[i].im);
+    if (w_out)
+        for (int64_t i = 0; i < op; i++) { w_out[2 * i] = v[i].re; w_out[2 * i + 1] = v[i].im; }
+    *mana_out = log2(s / (double)dim);
+    free(v);
+    return OR_OK;
+}
+
+/* ------------------------------------------------------------------------- */
+/* Adjoint (no reference counterpart): d SRE / d(Re psi, Im psi)              */
+/* ------------------------------------------------------------------------- */
+
+/* Differentiates the reference's forward definition (src/SRE.jl:509-540 build,
+ * FWHT, sum of (F^2)^q) directly: for each x, G_x = WHT(2q F^{2q-1}) and, with
+ * s = r ^ x, g_x(r) = X1[r] T1[s] + X2[r] T2[s] (T1 = X1 + X2, T2 = X2 - X1):
+ *   dm/dX1[r] += G(r) T1[s],  dm/dX2[r] += G(r) T2[s],
+ *   dm/dX1[s] += G(r) (X1[r] - X2[r]),  dm/dX2[s] += G(r) (X1[r] + X2[r]).
+ * dSRE = -dm / (m ln 2).  grad is interleaved (d/dRe, d/dIm). */
+int or_sre_grad(const double *psi, int n, double q, int nthreads, double *sre_out, double *grad) {
+    if (n < 1 || n > 22 || nthreads < 1) return OR_ERR_ARG;
+    sre_prep s;
+    if (sre_prep_init(&s, psi, n) != OR_OK) return OR_ERR_ARG;
+    const int64_t dim = s.dim;
+    double *gacc = calloc((size_t)nthreads * 2 * (size_t)dim, sizeof(double));
+    double *macc = calloc((size_t)nthreads, sizeof(double));
+#pragma omp parallel num_threads(nthreads)
+    {
+        int tid = omp_get_thread_num();
+        double *v = malloc(sizeof(double) * (size_t)dim);
+        double *G = malloc(sizeof(double) * (size_t)dim);
+        double *g = gacc + (size_t)tid * 2 * (size_t)dim;
+        double mloc = 0.0;
+#pragma omp for schedule(static)
+        for (int64_t x = 0; x < dim; x++) {
+            for (int64_t r = 0; r < dim; r++) {
+                uint64_t j = (uint64_t)r ^ (uint64_t)x;
+                v[r] = fma(s.X1[r], s.TMP1[j], s.X2[r] * s.TMP2[j]);
+            }
+            or_fwht(v, n);
+            for (int64_t k = 0; k < dim; k++) {
+                double F = v[k], p = F * F;
+                mloc += pow_q(p, q);
+                /* d/dF (F^2)^q = 2 q F^(2q-1) = 2 q p^(q-1) F */
+                G[k] = 2.0 * q * (q == 2.0 ? p : pow(p, q - 1.0)) * F;
+            }
+            or_fwht(G, n);
+            for (int64_t r = 0; r < dim; r++) {
+                uint64_t sidx = (uint64_t)r ^ (uint64_t)x;
+                double gr = G[r];
+                g[2 * r] += gr * s.TMP1[sidx];
+                g[2 * r + 1] += gr * s.TMP2[sidx];
+                g[2 * sidx] += gr * (s.X1[r] - s.X2[r]);
+                g[2 * sidx + 1] += gr * (s.X1[r] + s.X2[r]);
+            }
+        }
+        macc[tid] = mloc;
+        free(v);
+        free(G);
+    }
+    double m = 0.0;
+    for (int t = 0; t < nthreads; t++) m += macc[t];
+    const double scale = -1.0 / (m * log(2.0));
+    for (int64_t i = 0; i < 2 * dim; i++) {
+        double a = 0.0;
+        for (int t = 0; t < nthreads; t++) a += gacc[(size_t)t * 2 * (size_t)dim + (size_t)i];
+        grad[i] = scale * a;
+    }
+    *sre_out = -log2(m / (double)dim);
+    free(gacc);
+    free(macc);
+    sre_prep_free(&s);
+    return OR_OK;
+}
