@@ -31,8 +31,11 @@ PRECISIONS = {"fp64": HM_FP64, "fp32": HM_FP32, "plain": HM_PLAIN}
 EXPORTS = [
     "hm_abi_version", "hm_create", "hm_destroy", "hm_last_error", "hm_set_stream", "hm_last_kernel_ms",
     "hm_sre", "hm_sre_dev", "hm_sre_range", "hm_sre_range_dev", "hm_sre_batched", "hm_sre_grad",
-    "hm_mc_sre", "hm_mana_pure", "hm_mana_mixed", "hm_gray_table", "hm_gray_table_general",
+    "hm_mc_sre", "hm_mana_pure", "hm_mana_mixed", "hm_gray_table", "hm_gray_table_general", "hm_set_param",
 ]
+HM_PARAM_BATCH = 1
+HM_PARAM_RING = 2
+HM_PARAM_UNITS = 3
 
 
 class ArgumentError(ValueError):
@@ -83,6 +86,7 @@ def load_library(path=None):
         L.hm_mana_mixed.argtypes = [_vp, _dp, i, _dp]
         L.hm_gray_table.argtypes = [_vp, i, _u64p, _i64p]
         L.hm_gray_table_general.argtypes = [_vp, i, i, _i64p, _i64p]
+        L.hm_set_param.argtypes = [i, i]
         for name in EXPORTS:
             if name != "hm_last_error" and name != "hm_abi_version":
                 getattr(L, name).restype = i
@@ -267,6 +271,13 @@ def _log3_exact(size):
     if t != 1:
         raise ArgumentError(f"length(vec)={size} is not a power of q=3")
     return n
+
+
+def set_param(param, value):
+    """Process-wide tuning knob (HM_PARAM_BATCH / HM_PARAM_RING); 0 restores the default."""
+    rc = load_library().hm_set_param(int(param), int(value))
+    if rc != HM_OK:
+        raise ArgumentError(f"hm_set_param({param}, {value}) rejected")
 
 
 _default_ctx = {}

@@ -17,6 +17,7 @@ struct hm_ctx {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0.0;
+  double last_wait_frac = 0.0;  // two-pass sweep: share of CTA time in dependency waits
   std::string err;
 
   // grow-only device buffers

@@ -178,6 +178,8 @@ static int plain_one_q(hm_ctx *c, const double2 *psi, int n, uint64_t kb, uint64
   const int L = n;
   int B = 128;
   while (B > 1 && (double)B * N * 8.0 > 16.0 * (1ull << 30)) B >>= 1;
+  if ((uint64_t)B > ke - kb) B = (int)(ke - kb);
+  if (B < 1) B = 1;
   const int threads = PLAIN_THREADS;
   const int blocks_x = (int)std::min<uint64_t>(1024, (N + threads * 2 - 1) / (threads * 2));
   HM_TRY(ensure_dev(c, &c->d_inter, &c->inter_cap, (size_t)B * N * sizeof(double)));

@@ -216,95 +216,119 @@ __device__ __forceinline__ double q_scale(int t, bool xzero, const QParams &qp) 
 }
 
 // ---------------------------------------------------------------------------------
-// X-string bookkeeping for the two-pass engine
+// X-string bookkeeping for the two-pass engine.  Pass 1 pairs rows of the high index
+// part, so the pairing bit jt of x must be >= PB.  For 1 <= x < 2^PB the kernel reads a
+// copy of psi with bits j (the highest set bit of x) and n-1 swapped, on which the
+// relabelled string xt = x ^ 2^j ^ 2^(n-1) has its pairing bit at n-1.  x = 0 is not
+// handled by the two-pass kernel (its F is the plain transform of |psi|^2).
 struct XInfo {
   uint64_t xt;  // effective x after the relabelling (pairing bit in the high part)
   int jt;       // pairing bit of xt
-  int sw;       // relabelling: swap bit sw with bit n-1 (or -1)
-  int zero;     // x == 0
-  int active;   // Gray index inside the requested range
+  int sw;       // relabelling: read the copy with bits sw and n-1 swapped (or -1)
+  int active;   // Gray index inside the requested range and x != 0
 };
 
 __device__ __forceinline__ XInfo make_xinfo(uint64_t k, uint64_t k_end, int n, int pb) {
   XInfo xi;
-  xi.active = k < k_end;
   const uint64_t x = gray_code(k);
-  xi.zero = (x == 0);
+  xi.active = (k < k_end) && (x != 0);
   xi.sw = -1;
-  if (x == 0) {
-    xi.xt = 1ull << (n - 1);
+  xi.xt = x;
+  xi.jt = x ? 63 - __clzll((long long)x) : n - 1;
+  if (x != 0 && xi.jt < pb) {
+    xi.sw = xi.jt;
+    xi.xt = (x ^ (1ull << xi.jt)) | (1ull << (n - 1));
     xi.jt = n - 1;
-  } else {
-    const int j = 63 - __clzll((long long)x);
-    if (j >= pb) {
-      xi.xt = x;
-      xi.jt = j;
-    } else {
-      xi.xt = (x ^ (1ull << j)) | (1ull << (n - 1));
-      xi.jt = n - 1;
-      xi.sw = j;
-    }
   }
   return xi;
 }
 
-// Pass 1: gather + build row rho of the (n-1)-bit index of x, transform its low PB
-// bits, store it in layout-A order (position p = 32 i + l for the value of register i
-// of lane l, i.e. element k = R l + i).
-template <int R, bool ZERO, bool SWAP, typename V>
-__device__ __forceinline__ void p1_build(V (&v)[R], const V *__restrict__ psi, int n, const XInfo &xi,
-                                         uint64_t rho, int lane) {
+// Pass 1: gather + build row rho of the (n-1)-bit index of x and transform its low PB
+// bits.  The conj side a = psi(row rH) is loaded straight into the registers that will
+// hold f; the partner row b = psi(row sH) goes to the warp's shared buffer through
+// cp.async (no registers held while in flight), is read back permuted by the low bits
+// of x, and the buffer is then reused for the transpose.
+__device__ __forceinline__ void cp_async16(void *smem_dst, const void *gmem_src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *smem_dst, const void *gmem_src) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(s), "l"(gmem_src) : "memory");
+}
+template <typename V>
+__device__ __forceinline__ void cp_async_v(V *smem_dst, const V *gmem_src) {
+  if constexpr (sizeof(V) == 16)
+    cp_async16(smem_dst, gmem_src);
+  else
+    cp_async8(smem_dst, gmem_src);
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
+template <int R, bool STAGE_B, typename V>
+__device__ __forceinline__ void p1_build(V (&v)[R], const V *__restrict__ psi, const XInfo &xi, uint64_t rho, V *sm,
+                                         int lane) {
   constexpr int PB = ilog2c(R) + 5;
   const uint64_t rH = insert0(rho, xi.jt - PB);
   const uint64_t sH = rH ^ (xi.xt >> PB);
   const uint32_t xL = (uint32_t)(xi.xt & ((1ull << PB) - 1ull));
-  const uint64_t baseA = rH << PB, baseB = sH << PB;
+  const V *rowA = psi + (rH << PB);
+  const V *rowB = psi + (sH << PB);
+  if constexpr (STAGE_B) {
+    // partner row, in natural order, into the shared buffer
 #pragma unroll
-  for (int i = 0; i < R; ++i) {
-    const uint32_t e = (uint32_t)(i * 32 + lane);
-    uint64_t ra = baseA | e, rb = baseB | (e ^ xL);
-    if (SWAP) {
-      ra = swap_bits(ra, xi.sw, n - 1);
-      rb = swap_bits(rb, xi.sw, n - 1);
+    for (int i = 0; i < R; ++i) cp_async_v(sm + i * 32 + lane, rowB + i * 32 + lane);
+    // conj side straight into registers
+#pragma unroll
+    for (int i = 0; i < R; ++i) v[i] = ld_psi(rowA + i * 32 + lane);
+    cp_async_wait_all();
+    __syncwarp();
+#pragma unroll
+    for (int i = 0; i < R; ++i) v[i] = conj_mul(v[i], sm[(uint32_t)(i * 32 + lane) ^ xL]);
+    __syncwarp();  // the buffer is rewritten by the transpose
+  } else {
+    // both rows straight into registers (the partner permuted by the low bits of x)
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const uint32_t e = (uint32_t)(i * 32 + lane);
+      v[i] = conj_mul(ld_psi(rowA + e), ld_psi(rowB + (e ^ xL)));
     }
-    const V a = ld_psi(psi + ra), b = ld_psi(psi + rb);
-    v[i] = ZERO ? zero_pair(a, b) : conj_mul(a, b);
   }
 }
 
-template <int R, typename V>
-__device__ __forceinline__ void p1_unit(const V *__restrict__ psi, int n, const XInfo &xi, uint64_t rho,
-                                        V *__restrict__ out_row, V *sm, int lane) {
-  constexpr int LOGR = ilog2c(R);
+// Ring layout of one X-string's intermediate (2^(n-1) complex): tile-major,
+//   inter_x[t * 2^(HI+LOGC) + row * C + c]  for pass-2 tile t, row, column c < C,
+// so that a pass-2 tile is one contiguous 2^PB-element block and pass 1 writes whole
+// 32-byte sectors (C >= 2).
+template <int R, int HI, bool STAGE_B, typename V>
+__device__ __forceinline__ void p1_unit(const V *__restrict__ psi, const XInfo &xi, uint64_t rho,
+                                        V *__restrict__ inter_x, V *sm, int lane) {
+  constexpr int LOGR = ilog2c(R), PB = LOGR + 5, LOGC = PB - HI;
   V v[R];
-  if (xi.zero)
-    p1_build<R, true, false>(v, psi, n, xi, rho, lane);
-  else if (xi.sw >= 0)
-    p1_build<R, false, true>(v, psi, n, xi, rho, lane);
-  else
-    p1_build<R, false, false>(v, psi, n, xi, rho, lane);
+  p1_build<R, STAGE_B>(v, psi, xi, rho, sm, lane);
   reg_wht<R, 0, LOGR>(v);  // element bits 5 .. PB-1
   transpose_ab<R>(v, sm, lane);
   reg_wht<R, 0, 5>(v);  // element bits 0 .. 4
-#pragma unroll
-  for (int i = 0; i < R; ++i) __stcg(out_row + i * 32 + lane, v[i]);
-}
-
-// Pass 2: tile of 2^HI rows x C = 2^(PB-HI) consecutive positions of one X-string's
-// intermediate; transform over the row bits, then per-lane moments.
-template <int R, int HI, int QS, typename V>
-__device__ __forceinline__ void p2_unit(const V *__restrict__ inter_x, uint32_t tile, V *sm, int lane, double *s,
-                                        const QParams &qp) {
-  constexpr int LOGR = ilog2c(R), PB = LOGR + 5, LOGC = PB - HI, C = 1 << LOGC;
-  static_assert(HI >= 1 && HI <= PB, "pass-2 bits out of range");
-  V v[R];
-  const uint32_t p0 = tile * C;
+  // register i of lane l holds element k = R l + i; it is stored at position p = 32 i + l
+  // of the row (any fixed relabelling of k is invisible to the moment sums)
 #pragma unroll
   for (int i = 0; i < R; ++i) {
-    const uint32_t e = (uint32_t)(i * 32 + lane);
-    const uint32_t row = e >> LOGC, c = e & (C - 1);
-    v[i] = __ldcg(inter_x + (size_t)row * (32 * R) + p0 + c);
+    const uint32_t p = (uint32_t)(i * 32 + lane);
+    const uint32_t t = p >> LOGC, c = p & ((1u << LOGC) - 1u);
+    __stcg(inter_x + (((size_t)t << (HI + LOGC)) + (rho << LOGC) + c), v[i]);
   }
+}
+
+// Pass 2: tile of 2^HI rows x C = 2^(PB-HI) positions of one X-string's intermediate
+// (one contiguous block); transform over the row bits, then per-lane moments.
+template <int R, int HI, int QS, typename V>
+__device__ __forceinline__ void p2_unit(const V *__restrict__ tile_ptr, V *sm, int lane, double *s,
+                                        const QParams &qp) {
+  constexpr int LOGR = ilog2c(R), PB = LOGR + 5, LOGC = PB - HI;
+  static_assert(HI >= 1 && HI <= PB, "pass-2 bits out of range");
+  V v[R];
+#pragma unroll
+  for (int i = 0; i < R; ++i) v[i] = __ldcg(tile_ptr + i * 32 + lane);
   if constexpr (LOGC >= 5) {
     reg_wht<R, LOGC - 5, LOGR>(v);
   } else {

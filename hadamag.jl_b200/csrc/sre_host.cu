@@ -59,6 +59,16 @@ __global__ void k_psi_to_f32(const double2 *__restrict__ in, float2 *__restrict_
   }
 }
 
+// (hi, lo) += (b_hi, b_lo), Knuth TwoSum on the high parts
+static void dd_add_host(double *a, double bh, double bl) {
+  const double s = a[0] + bh;
+  const double bb = s - a[0];
+  const double err = (a[0] - (s - bb)) + (bh - bb);
+  const double lo = a[1] + bl + err;
+  a[0] = s + lo;
+  a[1] = lo - (a[0] - s);
+}
+
 // Map requested q values onto a kernel moment set.  Returns the kind and, per request,
 // the index of its sum in the kernel output (1-based; 0 is sum F^2).
 static int choose_qs(const QReq &q, QParams &qp, int *idx) {
@@ -119,12 +129,19 @@ int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, 
   unsigned *h_err = (unsigned *)(c->h_out + 14);
   *h_err = 0;
   const bool twopass = (n - 1) > 10;
-  if (twopass)
+  if (twopass) {
     HM_CUDA(c, cudaMemcpyAsync(h_err, c->d_ctrl + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    HM_CUDA(c, cudaMemcpyAsync(c->h_out + 12, c->d_ctrl + 4 + 2 * twopass_cfg().S, 2 * sizeof(unsigned long long),
+                               cudaMemcpyDeviceToHost, c->stream));
+  }
   HM_CUDA(c, cudaStreamSynchronize(c->stream));
   float ms = 0.f;
   HM_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
   c->last_ms = ms;
+  if (twopass) {
+    const unsigned long long *st = reinterpret_cast<const unsigned long long *>(c->h_out + 12);
+    c->last_wait_frac = st[1] ? (double)st[0] / (double)st[1] : 0.0;
+  }
   if (twopass && *h_err)
     return set_err(c, HM_ERR_TIMEOUT, "two-pass sweep: a dependency wait exceeded its limit; results invalid");
   out_dd[0] = c->h_out[0];
@@ -133,7 +150,62 @@ int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, 
     out_dd[2 + 2 * i] = c->h_out[2 * idx[i]];
     out_dd[3 + 2 * i] = c->h_out[2 * idx[i] + 1];
   }
+  if (twopass && kb == 0) {
+    // x = 0 (F = WHT of |psi|^2) is not part of the two-pass sweep: one FP64 transform
+    // through the plain path, added as a double-double term
+    const double ms_main = c->last_ms;
+    double z[10];
+    HM_TRY(run_sre_plain(c, psi_dev, n, 0, 1, q, z));
+    c->last_ms += ms_main;
+    for (int t = 0; t < 1 + q.nq; ++t) dd_add_host(out_dd + 2 * t, z[2 * t], z[2 * t + 1]);
+  }
   return HM_OK;
 }
 
 }  // namespace hm
+
+// fraction of CTA time spent in dependency waits during the last two-pass sweep
+extern "C" int hm_debug_wait_fraction(hm_ctx *c, double *out) {
+  if (!c || !out) return HM_ERR_ARG;
+  *out = c->last_wait_frac;
+  return HM_OK;
+}
+
+extern "C" int hm_set_param(int param, int value) {
+  hm::TwoPassCfg &cfg = hm::twopass_cfg();
+  if (param == HM_PARAM_BATCH) {
+    if (value == 0) {
+      cfg.X_set = 0;
+      return HM_OK;
+    }
+    if (value < 2 || value > 64 || (value & (value - 1))) return HM_ERR_ARG;
+    cfg.X = value;
+    cfg.X_set = 1;
+    return HM_OK;
+  }
+  if (param == 106) {  // pass-1 partner row through shared memory (experiments)
+    cfg.stage_b = value;
+    return HM_OK;
+  }
+  if (param == 105) {  // completion-signal flavour (experiments)
+    cfg.release = value;
+    return HM_OK;
+  }
+  if (param == 104) {  // per-lane fences on/off (experiments)
+    cfg.fence_all = value ? 1 : 0;
+    return HM_OK;
+  }
+  if (param == HM_PARAM_UNITS) {
+    if (value == 0) value = hm::TwoPassCfg().upw;
+    if (value < 1 || value > 64 || (value & (value - 1))) return HM_ERR_ARG;
+    cfg.upw = value;
+    return HM_OK;
+  }
+  if (param == HM_PARAM_RING) {
+    if (value == 0) value = hm::TwoPassCfg().S;
+    if (value < 2 || value > 8) return HM_ERR_ARG;
+    cfg.S = value;
+    return HM_OK;
+  }
+  return HM_ERR_ARG;
+}

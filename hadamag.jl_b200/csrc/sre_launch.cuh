@@ -11,7 +11,12 @@ namespace hm {
 // stays resident in the 126 MB L2 next to the 16 MiB state.
 struct TwoPassCfg {
   int X = 2;
+  int X_set = 0;  // X was set explicitly (otherwise 2 for FP64, 4 for FP32)
   int S = 3;
+  int upw = 1;  // warp units per warp per CTA item
+  int fence_all = 0;  // every lane fences its own stores before the completion signal
+  int release = 0;    // completion signal: 0 fence.sc + atomic, 1 red.release, 2 fence.acq_rel + atomic
+  int stage_b = 0;    // pass 1 stages the partner row through shared memory (cp.async)
 };
 
 TwoPassCfg &twopass_cfg();
@@ -54,20 +59,34 @@ static int launch_2pass(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
   int occ = 0;
   HM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, SRE_WARPS * 32, smem));
   if (occ < 1) occ = 1;
-  a.X = cfg.X;
+  // FP32 rows are half the bytes: twice the X-strings per batch fit the same L2 budget
+  a.X = cfg.X_set ? cfg.X : (sizeof(T) == 8 ? 2 : 4);
   a.S = cfg.S;
+  a.flags = (cfg.fence_all ? 2 : 0) | (cfg.release == 1 ? 4 : 0) | (cfg.release == 2 ? 8 : 0) | (cfg.stage_b ? 16 : 0);
   const uint64_t len = a.k_end - a.k_begin;
   a.nbatch = (int)((len + a.X - 1) / a.X);
   const uint64_t U = 1ull << HI;
-  const long long K = (long long)((a.X * U) / SRE_WARPS);
+  a.upw = cfg.upw;
+  while (a.upw > 1 && (uint64_t)a.X * U < (uint64_t)SRE_WARPS * a.upw) a.upw >>= 1;
+  const long long K = (long long)((a.X * U) / (SRE_WARPS * a.upw));  // CTA items per pass per batch
   a.nitems = 2 * K * (long long)a.nbatch;
   const size_t inter_bytes = (size_t)a.S * a.X * ((size_t)1 << (a.n - 1)) * sizeof(V);
   HM_TRY(ensure_dev(c, &c->d_inter, &c->inter_cap, inter_bytes));
   a.inter = c->d_inter;
-  const size_t ctrl_words = 4 + 2 * (size_t)a.S;
+  const size_t ctrl_words = 8 + 2 * (size_t)a.S;
   HM_TRY(ensure_dev(c, (void **)&c->d_ctrl, &c->ctrl_cap, ctrl_words * sizeof(unsigned)));
   HM_CUDA(c, cudaMemsetAsync(c->d_ctrl, 0, ctrl_words * sizeof(unsigned), c->stream));
   a.ctrl = c->d_ctrl;
+  // bit-swapped copies of psi for the X-strings 1 <= x < 2^PB (Gray indices below 2^PB)
+  constexpr int PB = ilog2c(R) + 5;
+  if (a.k_begin < (1ull << PB)) {
+    const size_t len = (size_t)1 << a.n;
+    HM_TRY(ensure_dev(c, &c->d_aux2, &c->aux2_cap, (size_t)PB * len * sizeof(V)));
+    k_psi_swapped<V><<<c->num_sms * 8, 256, 0, c->stream>>>(reinterpret_cast<const V *>(a.psi),
+                                                            reinterpret_cast<V *>(c->d_aux2), a.n, PB);
+    HM_CUDA(c, cudaGetLastError());
+    for (int j = 0; j < PB; ++j) a.psi_sw[j] = reinterpret_cast<const V *>(c->d_aux2) + (size_t)j * len;
+  }
   int blocks = c->num_sms * occ;
   if ((long long)blocks > a.nitems) blocks = (int)a.nitems;
   if (blocks < 1) blocks = 1;

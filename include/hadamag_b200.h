@@ -65,6 +65,16 @@ const char *hm_last_error(hm_ctx *ctx);
  * stream).  Lets a caller time the kernels with events on that stream. */
 int hm_set_stream(hm_ctx *ctx, void *cuda_stream);
 
+/* Tuning knobs of the exact-SRE sweeps (the autotuner sets them; defaults are used
+ * otherwise).  HM_PARAM_BATCH: X-strings per batch of the two-pass sweep (power of two,
+ * 2..64); HM_PARAM_RING: batches in flight in the L2 ring (2..8); HM_PARAM_UNITS:
+ * row/tile units each warp processes per work item (power of two, 1..64).  Value 0
+ * restores the default.  Process-wide. */
+#define HM_PARAM_BATCH 1
+#define HM_PARAM_RING 2
+#define HM_PARAM_UNITS 3
+int hm_set_param(int param, int value);
+
 /* Device time in milliseconds of the main kernels of the last call (CUDA events on the
  * context's stream, recorded around the launches that do the transform work). */
 int hm_last_kernel_ms(hm_ctx *ctx, double *ms);
