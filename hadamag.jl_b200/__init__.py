@@ -21,6 +21,7 @@ import warnings
 
 import numpy as np
 
+from . import shard  # noqa: F401  (multi-GPU Gray-range split)
 from ._native import (HM_FP32, HM_FP64, HM_PLAIN, PRECISIONS, ArgumentError, Context, HadaMAGError,
                       default_context, load_library)
 

@@ -32,10 +32,12 @@ EXPORTS = [
     "hm_abi_version", "hm_create", "hm_destroy", "hm_last_error", "hm_set_stream", "hm_last_kernel_ms",
     "hm_sre", "hm_sre_dev", "hm_sre_range", "hm_sre_range_dev", "hm_sre_batched", "hm_sre_grad",
     "hm_mc_sre", "hm_mana_pure", "hm_mana_mixed", "hm_gray_table", "hm_gray_table_general", "hm_set_param",
+    "hm_last_launch_count", "hm_probe_fp64_peak",
 ]
 HM_PARAM_BATCH = 1
 HM_PARAM_RING = 2
 HM_PARAM_UNITS = 3
+HM_PARAM_GRAPH = 4
 
 
 class ArgumentError(ValueError):
@@ -87,6 +89,8 @@ def load_library(path=None):
         L.hm_gray_table.argtypes = [_vp, i, _u64p, _i64p]
         L.hm_gray_table_general.argtypes = [_vp, i, i, _i64p, _i64p]
         L.hm_set_param.argtypes = [i, i]
+        L.hm_last_launch_count.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong)]
+        L.hm_probe_fp64_peak.argtypes = [_vp, _dp]
         for name in EXPORTS:
             if name != "hm_last_error" and name != "hm_abi_version":
                 getattr(L, name).restype = i
@@ -136,6 +140,16 @@ class Context:
 
     def set_stream(self, stream_handle):
         self._check(self.lib.hm_set_stream(self.handle, _vp(stream_handle or 0)), "hm_set_stream")
+
+    def last_launch_count(self):
+        v = ctypes.c_longlong()
+        self._check(self.lib.hm_last_launch_count(self.handle, ctypes.byref(v)), "hm_last_launch_count")
+        return v.value
+
+    def probe_fp64_peak(self):
+        v = ctypes.c_double()
+        self._check(self.lib.hm_probe_fp64_peak(self.handle, ctypes.byref(v)), "hm_probe_fp64_peak")
+        return v.value
 
     def last_kernel_ms(self):
         v = ctypes.c_double()

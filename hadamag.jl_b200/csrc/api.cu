@@ -92,6 +92,22 @@ __global__ void k_gray_general(int64_t *xtab, int64_t *flips, uint64_t N, int q,
   }
 }
 
+// eight independent DADD chains per thread; the result is only stored under a condition
+// that never holds, which keeps the chains live
+__global__ void k_probe_dadd(double *out, int iters, double s) {
+  double a[8];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) a[j] = threadIdx.x + j;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a[j] = a[j] + s;
+  }
+  double t = 0.0;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) t += a[j];
+  if (t == -1.0) out[0] = t;
+}
+
 }  // namespace
 
 extern "C" {
@@ -144,6 +160,30 @@ int hm_set_stream(hm_ctx *c, void *stream) {
   return HM_OK;
 }
 
+int hm_last_launch_count(hm_ctx *c, long long *count) {
+  if (!c || !count) return HM_ERR_ARG;
+  *count = c->launches;
+  return HM_OK;
+}
+
+int hm_probe_fp64_peak(hm_ctx *c, double *ops_per_s) {
+  if (!c || !ops_per_s) return HM_ERR_ARG;
+  c->err.clear();
+  HM_CUDA(c, cudaSetDevice(c->device));
+  HM_TRY(ensure_dev(c, (void **)&c->d_out, &c->out_cap, sizeof(double) * 16));
+  const int blocks = c->num_sms * 8, threads = 256, iters = 8192;
+  k_probe_dadd<<<blocks, threads, 0, c->stream>>>(c->d_out, 64, 1.0);  // warm-up
+  HM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+  k_probe_dadd<<<blocks, threads, 0, c->stream>>>(c->d_out, iters, 1.0);
+  HM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+  HM_CUDA(c, cudaGetLastError());
+  HM_CUDA(c, cudaEventSynchronize(c->ev1));
+  float ms = 0.f;
+  HM_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  *ops_per_s = (double)blocks * threads * iters * 8.0 / (ms * 1e-3);
+  return HM_OK;
+}
+
 int hm_last_kernel_ms(hm_ctx *c, double *ms) {
   if (!c || !ms) return HM_ERR_ARG;
   *ms = c->last_ms;
@@ -154,6 +194,7 @@ int hm_sre_range_dev(hm_ctx *c, const double *psi_dev, int n, uint64_t kb, uint6
                      int precision, double *p2_dd, double *m_dd) {
   if (!c) return HM_ERR_ARG;
   c->err.clear();
+  c->launches = 0;
   if (!p2_dd || !m_dd) return set_err(c, HM_ERR_ARG, "null output pointer");
   if (n < 1 || n > 24) return set_err(c, HM_ERR_SIZE, "n = %d outside [1, 24]", n);
   const uint64_t dim = 1ull << n;
@@ -213,6 +254,46 @@ int hm_sre(hm_ctx *c, const double *psi, int n, const double *qs, int nq, int pr
   const double2 *d;
   HM_TRY(stage_psi(c, psi, 1ull << n, &d));
   return hm_sre_dev(c, (const double *)d, n, qs, nq, precision, out_sre, out_lost);
+}
+
+int hm_sre_batched(hm_ctx *c, int nstates, const double *const *psis, const int *ns, const double *qs, int nq,
+                   int precision, double *out_sre, double *out_lost) {
+  if (!c) return HM_ERR_ARG;
+  c->err.clear();
+  if (nstates < 0 || (nstates > 0 && (!psis || !ns || !out_sre || !out_lost)))
+    return set_err(c, HM_ERR_ARG, "null pointer or negative state count");
+  QReq q;
+  HM_TRY(check_qs(c, qs, nq, q));
+  HM_TRY(check_prec(c, precision));
+  size_t total = 0;
+  for (int s = 0; s < nstates; ++s) {
+    if (!psis[s]) return set_err(c, HM_ERR_ARG, "state %d: null pointer", s);
+    if (ns[s] < 1 || ns[s] > 24) return set_err(c, HM_ERR_SIZE, "state %d: n = %d outside [1, 24]", s, ns[s]);
+    total += (size_t)1 << ns[s];
+  }
+  HM_CUDA(c, cudaSetDevice(c->device));
+  // every state goes to the device in one staging buffer, then the states run back to
+  // back on the context's stream
+  HM_TRY(ensure_dev(c, &c->d_psi, &c->psi_cap, total * sizeof(double2)));
+  size_t off = 0;
+  for (int s = 0; s < nstates; ++s) {
+    const size_t len = (size_t)1 << ns[s];
+    HM_CUDA(c, cudaMemcpyAsync((double2 *)c->d_psi + off, psis[s], len * sizeof(double2), cudaMemcpyHostToDevice,
+                               c->stream));
+    off += len;
+  }
+  off = 0;
+  double total_ms = 0.0;
+  for (int s = 0; s < nstates; ++s) {
+    const size_t len = (size_t)1 << ns[s];
+    double dd[10];
+    HM_TRY(run_sre(c, (const double2 *)c->d_psi + off, ns[s], 0, len, q, precision, dd));
+    total_ms += c->last_ms;
+    sre_finish(dd, ns[s], nq, out_sre + (size_t)s * nq, out_lost + s);
+    off += len;
+  }
+  c->last_ms = total_ms;
+  return HM_OK;
 }
 
 int hm_gray_table(hm_ctx *c, int n, uint64_t *codes, int64_t *flips) {

@@ -70,33 +70,4 @@ __device__ __forceinline__ uint64_t swap_bits(uint64_t r, int a, int b) {
   return r ^ (d << a) ^ (d << b);
 }
 
-// acquire load / release add at GPU scope for the inter-CTA dependency counters
-__device__ __forceinline__ unsigned ld_acquire_gpu(const unsigned *p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-__device__ __forceinline__ void red_release_gpu_add(unsigned *p, unsigned v) {
-  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
-}
-
-// Bounded wait until *counter >= target.  Returns false (and raises *err) after
-// `limit` clock cycles; never spins unboundedly.
-__device__ __forceinline__ bool wait_counter(const unsigned *counter, unsigned target, unsigned *err,
-                                             long long limit) {
-  if (ld_acquire_gpu(counter) >= target) return true;
-  const long long t0 = clock64();
-  unsigned ns = 32;
-  while (ld_acquire_gpu(counter) < target) {
-    if (*(volatile unsigned *)err) return false;
-    if (clock64() - t0 > limit) {
-      atomicExch(err, 1u);
-      return false;
-    }
-    __nanosleep(ns);
-    if (ns < 512) ns <<= 1;
-  }
-  return true;
-}
-
 }  // namespace hm

@@ -17,7 +17,7 @@ struct hm_ctx {
   cudaStream_t stream = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   double last_ms = 0.0;
-  double last_wait_frac = 0.0;  // two-pass sweep: share of CTA time in dependency waits
+  long long launches = 0;  // kernels launched by the current / last call
   std::string err;
 
   // grow-only device buffers
@@ -29,7 +29,7 @@ struct hm_ctx {
   size_t inter_cap = 0;
   double *d_partials = nullptr;
   size_t partials_cap = 0;
-  unsigned *d_ctrl = nullptr;  // queue + error flag + dependency counters
+  unsigned *d_ctrl = nullptr;  // stage index of the two-pass stage kernels
   size_t ctrl_cap = 0;
   double *d_out = nullptr;  // fold output
   size_t out_cap = 0;

@@ -1,0 +1,431 @@
+// mana.cu -- qutrit Mana kernels.
+//
+// Pure states (src/Mana.jl:19-92, src/Backends/Threads.jl:378-426).  For every ternary
+// X-string x the reference forms
+//     v(r) = conj psi(r (+) x) * (psi((-r) (+) x) / 3^L)        ((+): digitwise addition mod 3)
+// applies the qutrit Hadamard H3^{(x)L} (src/Helpers.jl:249-292) and sums |W|; the Mana
+// is log2(S) / log2(3).  The sum over x does not depend on the order in which the
+// X-strings are visited, so x runs over 0 .. 3^L - 1 directly.
+//
+// The 3^L-point transform is split like the exact-SRE sweep: the low `lo` digits of r
+// form a contiguous row (pass 1: gather + build + transform in shared memory), the high
+// `hi` digits a strided column (pass 2: transform + sum |W|).  Batches of X-strings keep
+// the intermediate resident in L2.  FP64 throughout.
+//
+// Mixed states (src/Mana.jl:123-314): w = M^{(x)N} vec9(rho) leg by leg, then
+// log2(sum |w| / 3^N).
+#include <math.h>
+
+#include "hm_common.cuh"
+#include "hm_ctx.h"
+
+namespace hm {
+
+namespace {
+
+constexpr int MANA_THREADS = 256;
+
+__host__ __device__ inline int ipow3(int e) {
+  int r = 1;
+  for (int i = 0; i < e; ++i) r *= 3;
+  return r;
+}
+
+// digitwise (a (+) b) and ((-a) (+) b) for numbers of `nd` base-3 digits
+__device__ inline int tadd(int a, int b, int nd) {
+  int r = 0, p = 1;
+  for (int i = 0; i < nd; ++i) {
+    r += ((a % 3 + b % 3) % 3) * p;
+    a /= 3;
+    b /= 3;
+    p *= 3;
+  }
+  return r;
+}
+__device__ inline int tnegadd(int a, int b, int nd) {
+  int r = 0, p = 1;
+  for (int i = 0; i < nd; ++i) {
+    r += (((3 - a % 3) % 3 + b % 3) % 3) * p;
+    a /= 3;
+    b /= 3;
+    p *= 3;
+  }
+  return r;
+}
+
+// the reference's 3-point DFT (a, b, c) -> (a+b+c, a+w b+w^2 c, a+w^2 b+w c), w = e^{2 pi i/3}
+__device__ __forceinline__ void dft3(double2 &a, double2 &b, double2 &c) {
+  const double wr = -0.5, wi = 0.86602540378443864676;  // cos, sin of 2 pi / 3
+  const double r0 = a.x + b.x + c.x, i0 = a.y + b.y + c.y;
+  const double r1 = a.x + wr * (b.x + c.x) - wi * (b.y - c.y);
+  const double i1 = a.y + wr * (b.y + c.y) + wi * (b.x - c.x);
+  const double r2 = a.x + wr * (b.x + c.x) + wi * (b.y - c.y);
+  const double i2 = a.y + wr * (b.y + c.y) - wi * (b.x - c.x);
+  a = make_double2(r0, i0);
+  b = make_double2(r1, i1);
+  c = make_double2(r2, i2);
+}
+
+// H3 over `nd` digits of a set of `nvec` vectors stored at sm[v * vstride + e * estride],
+// e in [0, 3^nd)
+__device__ void h3_smem(double2 *sm, int nd, int nvec, int vstride, int estride) {
+  const int len = ipow3(nd);
+  int step = 1;
+  for (int d = 0; d < nd; ++d) {
+    const int groups = len / 3;  // butterflies per vector per stage
+    for (int t = threadIdx.x; t < nvec * groups; t += blockDim.x) {
+      const int v = t / groups, g = t % groups;
+      const int blk = g / step, off = g % step;
+      const int i0 = blk * 3 * step + off;
+      double2 *base = sm + v * vstride;
+      double2 a = base[i0 * estride], b = base[(i0 + step) * estride], c = base[(i0 + 2 * step) * estride];
+      dft3(a, b, c);
+      base[i0 * estride] = a;
+      base[(i0 + step) * estride] = b;
+      base[(i0 + 2 * step) * estride] = c;
+    }
+    __syncthreads();
+    step *= 3;
+  }
+}
+
+struct ManaArgs {
+  const double2 *psi;
+  double2 *inter;  // batch x RH x RL
+  double *slots;   // per pass-2 CTA slot: dd (2 doubles)
+  int L, lo, hi, RL, RH, rows_per_cta, cols_per_cta;
+  int x0, nx;  // X-strings of this batch: x0 .. x0 + nx - 1
+  double invdim;
+};
+
+// pass 1: rows [blockIdx.x * rows_per_cta, ...) of X-string x0 + blockIdx.y
+__global__ void __launch_bounds__(MANA_THREADS) k_mana_p1(ManaArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double2 *sm = reinterpret_cast<double2 *>(smraw);
+  int *addL = reinterpret_cast<int *>(sm + a.rows_per_cta * a.RL);
+  int *negL = addL + a.RL;
+  const int xi = blockIdx.y;
+  if (xi >= a.nx) return;
+  const int x = a.x0 + xi;
+  const int xL = x % a.RL, xH = x / a.RL;
+  for (int e = threadIdx.x; e < a.RL; e += blockDim.x) {
+    addL[e] = tadd(e, xL, a.lo);
+    negL[e] = tnegadd(e, xL, a.lo);
+  }
+  __syncthreads();
+  const int row0 = blockIdx.x * a.rows_per_cta;
+  const int nrows = min(a.rows_per_cta, a.RH - row0);
+  for (int t = threadIdx.x; t < nrows * a.RL; t += blockDim.x) {
+    const int rr = t / a.RL, e = t % a.RL;
+    const int rH = row0 + rr;
+    const int cH = tadd(rH, xH, a.hi), dH = tnegadd(rH, xH, a.hi);
+    const double2 p = a.psi[(size_t)cH * a.RL + addL[e]];
+    double2 q = a.psi[(size_t)dH * a.RL + negL[e]];
+    q.x *= a.invdim;
+    q.y *= a.invdim;
+    sm[rr * a.RL + e] = make_double2(p.x * q.x + p.y * q.y, p.x * q.y - p.y * q.x);  // conj(p) * q
+  }
+  __syncthreads();
+  h3_smem(sm, a.lo, nrows, a.RL, 1);
+  double2 *out = a.inter + ((size_t)xi * a.RH + row0) * a.RL;
+  for (int t = threadIdx.x; t < nrows * a.RL; t += blockDim.x) out[t] = sm[t];
+}
+
+// pass 2: columns [blockIdx.x * cols_per_cta, ...) of X-string x0 + blockIdx.y; adds the
+// CTA's sum |W| into its double-double slot
+__global__ void __launch_bounds__(MANA_THREADS) k_mana_p2(ManaArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  double2 *sm = reinterpret_cast<double2 *>(smraw);
+  __shared__ double red[MANA_THREADS];
+  const int xi = blockIdx.y;
+  const int c0 = blockIdx.x * a.cols_per_cta;
+  const int ncols = min(a.cols_per_cta, a.RL - c0);
+  const double2 *in = a.inter + (size_t)xi * a.RH * a.RL;
+  if (xi < a.nx) {
+    // sm[col * RH + rH]
+    for (int t = threadIdx.x; t < a.RH * ncols; t += blockDim.x) {
+      const int rH = t / ncols, col = t % ncols;
+      sm[col * a.RH + rH] = in[(size_t)rH * a.RL + c0 + col];
+    }
+  }
+  __syncthreads();
+  if (xi < a.nx) h3_smem(sm, a.hi, ncols, a.RH, 1);
+  double s = 0.0;
+  if (xi < a.nx)
+    for (int t = threadIdx.x; t < a.RH * ncols; t += blockDim.x) s += hypot(sm[t].x, sm[t].y);
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    double *slot = a.slots + 2 * ((size_t)blockIdx.y * gridDim.x + blockIdx.x);
+    dd acc{slot[0], slot[1]};
+    dd_add(acc, red[0]);
+    slot[0] = acc.hi;
+    slot[1] = acc.lo;
+  }
+}
+
+__global__ void k_fold_dd(const double *slots, int nslots, double *out) {
+  __shared__ dd sh[256];
+  dd acc{0.0, 0.0};
+  for (int i = threadIdx.x; i < nslots; i += blockDim.x) dd_add_dd(acc, dd{slots[2 * i], slots[2 * i + 1]});
+  sh[threadIdx.x] = acc;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) dd_add_dd(sh[threadIdx.x], sh[threadIdx.x + o]);
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    out[0] = sh[0].hi;
+    out[1] = sh[0].lo;
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// mixed states
+struct M9 {
+  double2 m[81];
+};
+
+// vec9 (src/Mana.jl:190-228): v[p] = rho[r0 + dim * c0], the base-9 digit of p for site k
+// (site 1 most significant) being 3 i_k + j_k with i_k / j_k the k-th most significant
+// ternary digits of r0 / c0
+__global__ void k_vec_rho(const double2 *__restrict__ rho, double2 *__restrict__ v, int N, int dim, int op) {
+  for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < op; p += gridDim.x * blockDim.x) {
+    int t = p, r0 = 0, c0 = 0, w = 1;
+    for (int k = 0; k < N; ++k) {  // least significant base-9 digit first = site N
+      const int d9 = t % 9;
+      t /= 9;
+      r0 += (d9 / 3) * w;
+      c0 += (d9 % 3) * w;
+      w *= 3;
+    }
+    v[p] = rho[(size_t)r0 + (size_t)dim * c0];
+  }
+}
+
+// one leg of M^{(x)N} (src/Mana.jl:236-281): y = M x on every fiber of stride 9^(N-leg)
+__global__ void k_mana_leg(double2 *v, int op, int stride, M9 M) {
+  const int nfib = op / 9;
+  for (int f = blockIdx.x * blockDim.x + threadIdx.x; f < nfib; f += gridDim.x * blockDim.x) {
+    const int blk = f / stride, ofs = f % stride;
+    const size_t base = (size_t)blk * stride * 9 + ofs;
+    double2 x[9];
+#pragma unroll
+    for (int a = 0; a < 9; ++a) x[a] = v[base + (size_t)a * stride];
+#pragma unroll
+    for (int r = 0; r < 9; ++r) {
+      double sr = 0.0, si = 0.0;
+#pragma unroll
+      for (int c = 0; c < 9; ++c) {
+        const double2 m = M.m[9 * r + c];
+        sr += m.x * x[c].x - m.y * x[c].y;
+        si += m.x * x[c].y + m.y * x[c].x;
+      }
+      v[base + (size_t)r * stride] = make_double2(sr, si);
+    }
+  }
+}
+
+__global__ void k_abs_sum_slots(const double2 *v, int len, double *slots) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < len; i += gridDim.x * blockDim.x) s += hypot(v[i].x, v[i].y);
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    slots[2 * blockIdx.x] = red[0];
+    slots[2 * blockIdx.x + 1] = 0.0;
+  }
+}
+
+// host: the single-qutrit phase-point matrix of src/Mana.jl:123-182.  Row idx = 3a + a' is
+// the column-major vec of A_u^T with A_u = T_u A0 T_u^dagger, T_{a,a'} = w^{(-2 a a') mod 3}
+// Z^a X^{a'}, A0 = (1/3) sum_u T_u, X|k> = |k+1>, Z = diag(w^k).
+struct C {
+  double r, i;
+};
+static C cm(C a, C b) { return {a.r * b.r - a.i * b.i, a.r * b.i + a.i * b.r}; }
+static C ca(C a, C b) { return {a.r + b.r, a.i + b.i}; }
+static void m3(const C *A, const C *B, C *out) {
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) {
+      C s{0, 0};
+      for (int k = 0; k < 3; ++k) s = ca(s, cm(A[3 * i + k], B[3 * k + j]));
+      out[3 * i + j] = s;
+    }
+}
+static M9 phase_point_matrix() {
+  const double PI = 3.14159265358979323846;
+  const C w{cos(2 * PI / 3), sin(2 * PI / 3)};
+  C X[9] = {}, Z[9] = {}, I[9] = {};
+  const C wk[3] = {{1, 0}, w, cm(w, w)};
+  for (int k = 0; k < 3; ++k) {
+    X[3 * ((k + 1) % 3) + k] = {1, 0};
+    Z[3 * k + k] = wk[k];
+    I[3 * k + k] = {1, 0};
+  }
+  C Zp[3][9], Xp[3][9];
+  for (int i = 0; i < 9; ++i) {
+    Zp[0][i] = I[i];
+    Zp[1][i] = Z[i];
+    Xp[0][i] = I[i];
+    Xp[1][i] = X[i];
+  }
+  m3(Z, Z, Zp[2]);
+  m3(X, X, Xp[2]);
+  C T[9][9];
+  for (int a = 0; a < 3; ++a)
+    for (int ap = 0; ap < 3; ++ap) {
+      const int e = ((-2 * a * ap) % 3 + 3) % 3;
+      C ph{1, 0};
+      for (int t = 0; t < e; ++t) ph = cm(ph, w);
+      C zx[9];
+      m3(Zp[a], Xp[ap], zx);
+      for (int i = 0; i < 9; ++i) T[3 * a + ap][i] = cm(ph, zx[i]);
+    }
+  C A0[9] = {};
+  for (int u = 0; u < 9; ++u)
+    for (int i = 0; i < 9; ++i) A0[i] = ca(A0[i], T[u][i]);
+  for (int i = 0; i < 9; ++i) A0[i] = {A0[i].r / 3.0, A0[i].i / 3.0};
+  M9 M;
+  for (int u = 0; u < 9; ++u) {
+    C Td[9], tmp[9], Au[9];
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) Td[3 * i + j] = {T[u][3 * j + i].r, -T[u][3 * j + i].i};
+    m3(T[u], A0, tmp);
+    m3(tmp, Td, Au);
+    for (int i = 0; i < 3; ++i)
+      for (int j = 0; j < 3; ++j) M.m[9 * u + (i + 3 * j)] = make_double2(Au[3 * j + i].r, Au[3 * j + i].i);
+  }
+  return M;
+}
+
+}  // namespace
+
+int run_mana_pure(hm_ctx *c, const double2 *psi, int L, double *sum_dd) {
+  const int D = ipow3(L);
+  const int lo = (L + 1) / 2, hi = L - lo;
+  ManaArgs a;
+  a.psi = psi;
+  a.L = L;
+  a.lo = lo;
+  a.hi = hi;
+  a.RL = ipow3(lo);
+  a.RH = ipow3(hi);
+  a.rows_per_cta = std::max(1, 2048 / a.RL);
+  if (a.rows_per_cta > a.RH) a.rows_per_cta = a.RH;
+  a.cols_per_cta = std::max(1, std::min(a.RL, 2048 / a.RH));
+  a.invdim = 1.0 / (double)D;
+  // X-strings per batch: intermediate of at most 32 MiB (L2 resident)
+  int B = (int)std::max<size_t>(1, ((size_t)32 << 20) / ((size_t)D * sizeof(double2)));
+  if (B > D) B = D;
+  HM_TRY(ensure_dev(c, &c->d_inter, &c->inter_cap, (size_t)B * D * sizeof(double2)));
+  a.inter = (double2 *)c->d_inter;
+  const int g1 = (a.RH + a.rows_per_cta - 1) / a.rows_per_cta;
+  const int g2 = (a.RL + a.cols_per_cta - 1) / a.cols_per_cta;
+  const size_t nslots = (size_t)g2 * B;
+  HM_TRY(ensure_dev(c, (void **)&c->d_partials, &c->partials_cap, nslots * 2 * sizeof(double)));
+  HM_CUDA(c, cudaMemsetAsync(c->d_partials, 0, nslots * 2 * sizeof(double), c->stream));
+  a.slots = c->d_partials;
+  const size_t sm1 = (size_t)a.rows_per_cta * a.RL * sizeof(double2) + 2 * a.RL * sizeof(int);
+  const size_t sm2 = (size_t)a.cols_per_cta * a.RH * sizeof(double2);
+  HM_CUDA(c, cudaFuncSetAttribute(k_mana_p1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+  HM_CUDA(c, cudaFuncSetAttribute(k_mana_p2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+  HM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+  for (int x0 = 0; x0 < D; x0 += B) {
+    a.x0 = x0;
+    a.nx = std::min(B, D - x0);
+    k_mana_p1<<<dim3(g1, a.nx), MANA_THREADS, sm1, c->stream>>>(a);
+    k_mana_p2<<<dim3(g2, B), MANA_THREADS, sm2, c->stream>>>(a);
+  }
+  HM_CUDA(c, cudaGetLastError());
+  HM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+  HM_TRY(ensure_dev(c, (void **)&c->d_out, &c->out_cap, sizeof(double) * 16));
+  k_fold_dd<<<1, 256, 0, c->stream>>>(c->d_partials, (int)nslots, c->d_out);
+  HM_TRY(ensure_host(c, (void **)&c->h_out, &c->h_out_cap, sizeof(double) * 24));
+  HM_CUDA(c, cudaMemcpyAsync(c->h_out, c->d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  HM_CUDA(c, cudaStreamSynchronize(c->stream));
+  float ms = 0.f;
+  HM_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  c->last_ms = ms;
+  sum_dd[0] = c->h_out[0];
+  sum_dd[1] = c->h_out[1];
+  return HM_OK;
+}
+
+int run_mana_mixed(hm_ctx *c, const double2 *rho, int N, double *sum_dd) {
+  const int dim = ipow3(N);
+  int op = 1;
+  for (int i = 0; i < N; ++i) op *= 9;
+  HM_TRY(ensure_dev(c, &c->d_inter, &c->inter_cap, (size_t)op * sizeof(double2)));
+  double2 *v = (double2 *)c->d_inter;
+  const M9 M = phase_point_matrix();
+  HM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+  const int blocks = std::max(1, std::min((op + 255) / 256, c->num_sms * 8));
+  k_vec_rho<<<blocks, 256, 0, c->stream>>>(rho, v, N, dim, op);
+  for (int leg = 1; leg <= N; ++leg) {
+    int stride = 1;
+    for (int i = 0; i < N - leg; ++i) stride *= 9;
+    k_mana_leg<<<std::max(1, std::min((op / 9 + 127) / 128, c->num_sms * 8)), 128, 0, c->stream>>>(v, op, stride, M);
+  }
+  const int nb = std::max(1, std::min((op + 255) / 256, c->num_sms * 2));
+  HM_TRY(ensure_dev(c, (void **)&c->d_partials, &c->partials_cap, (size_t)nb * 2 * sizeof(double)));
+  k_abs_sum_slots<<<nb, 256, 0, c->stream>>>(v, op, c->d_partials);
+  HM_CUDA(c, cudaGetLastError());
+  HM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+  HM_TRY(ensure_dev(c, (void **)&c->d_out, &c->out_cap, sizeof(double) * 16));
+  k_fold_dd<<<1, 256, 0, c->stream>>>(c->d_partials, nb, c->d_out);
+  HM_TRY(ensure_host(c, (void **)&c->h_out, &c->h_out_cap, sizeof(double) * 24));
+  HM_CUDA(c, cudaMemcpyAsync(c->h_out, c->d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  HM_CUDA(c, cudaStreamSynchronize(c->stream));
+  float ms = 0.f;
+  HM_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  c->last_ms = ms;
+  sum_dd[0] = c->h_out[0];
+  sum_dd[1] = c->h_out[1];
+  return HM_OK;
+}
+
+}  // namespace hm
+
+extern "C" {
+
+int hm_mana_pure(hm_ctx *c, const double *psi, int L, double *out) {
+  if (!c) return HM_ERR_ARG;
+  c->err.clear();
+  if (!psi || !out) return hm::set_err(c, HM_ERR_ARG, "null pointer");
+  if (L < 1 || L > 12) return hm::set_err(c, HM_ERR_SIZE, "L = %d qutrits outside [1, 12]", L);
+  HM_CUDA(c, cudaSetDevice(c->device));
+  const size_t D = (size_t)hm::ipow3(L);
+  HM_TRY(hm::ensure_dev(c, &c->d_psi, &c->psi_cap, D * sizeof(double2)));
+  HM_CUDA(c, cudaMemcpyAsync(c->d_psi, psi, D * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+  double s[2];
+  HM_TRY(hm::run_mana_pure(c, (const double2 *)c->d_psi, L, s));
+  *out = log2(s[0] + s[1]) / log2(3.0);
+  return HM_OK;
+}
+
+int hm_mana_mixed(hm_ctx *c, const double *rho, int N, double *out) {
+  if (!c) return HM_ERR_ARG;
+  c->err.clear();
+  if (!rho || !out) return hm::set_err(c, HM_ERR_ARG, "null pointer");
+  if (N < 1 || N > 8) return hm::set_err(c, HM_ERR_SIZE, "N = %d qutrits outside [1, 8]", N);
+  HM_CUDA(c, cudaSetDevice(c->device));
+  const size_t dim = (size_t)hm::ipow3(N);
+  HM_TRY(hm::ensure_dev(c, &c->d_psi, &c->psi_cap, dim * dim * sizeof(double2)));
+  HM_CUDA(c, cudaMemcpyAsync(c->d_psi, rho, dim * dim * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+  double s[2];
+  HM_TRY(hm::run_mana_mixed(c, (const double2 *)c->d_psi, N, s));
+  *out = log2((s[0] + s[1]) / (double)dim);
+  return HM_OK;
+}
+
+}  // extern "C"

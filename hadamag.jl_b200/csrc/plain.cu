@@ -213,8 +213,10 @@ static int plain_one_q(hm_ctx *c, const double2 *psi, int n, uint64_t kb, uint64
       k_plain_last_reduce<<<gr, threads, 4 * threads * sizeof(double), c->stream>>>(X, N, 1ull << (L - 1), out_p2,
                                                                                     out_mq, q, q2);
     }
+    c->launches += 3 + (fuse == L ? 0 : (L - 1 - fuse));
     HM_CUDA(c, cudaGetLastError());
     k_plain_batch_fold<<<1, 256, 0, c->stream>>>(out_p2, out_mq, blocks_x * fill, c->d_out);
+    c->launches += 1;
     HM_CUDA(c, cudaMemcpyAsync(c->h_out, c->d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     HM_CUDA(c, cudaStreamSynchronize(c->stream));  // per-batch host fold, as the reference
     p2SAM += c->h_out[0];

@@ -111,46 +111,45 @@ int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, 
   if (precision == HM_FP32) {
     HM_TRY(ensure_dev(c, &c->d_psi32, &c->psi32_cap, len * sizeof(float2)));
     k_psi_to_f32<<<c->num_sms * 4, 256, 0, c->stream>>>(psi_dev, (float2 *)c->d_psi32, len);
+    c->launches += 1;
     HM_CUDA(c, cudaGetLastError());
     psi_k = c->d_psi32;
   }
+  // x = 0 (F = WHT of |psi|^2, whose F(0)^4 = 1 can dominate m) always runs as one FP64
+  // transform through the plain path: the two-pass kernels have no x = 0 build, and the
+  // FP32 kernels would round it
+  const bool split_zero = kb == 0 && ((n - 1) > 10 || precision == HM_FP32);
+  const uint64_t kb_main = split_zero ? 1 : kb;
   int nwarps = 0;
   HM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
-  if (precision == HM_FP32)
-    HM_TRY((launch_sre_prec<float>(c, psi_k, n, kb, ke, kind, qp, &nwarps)));
-  else
-    HM_TRY((launch_sre_prec<double>(c, psi_k, n, kb, ke, kind, qp, &nwarps)));
+  if (kb_main >= ke) {
+    // only x = 0 requested: the main kernels have nothing to do
+    HM_TRY(ensure_dev(c, (void **)&c->d_partials, &c->partials_cap, sizeof(double) * 16));
+    HM_CUDA(c, cudaMemsetAsync(c->d_partials, 0, sizeof(double) * 2 * nsum, c->stream));
+    nwarps = 1;
+  } else if (precision == HM_FP32) {
+    HM_TRY((launch_sre_prec<float>(c, psi_k, n, kb_main, ke, kind, qp, &nwarps)));
+  } else {
+    HM_TRY((launch_sre_prec<double>(c, psi_k, n, kb_main, ke, kind, qp, &nwarps)));
+  }
   HM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
   HM_TRY(ensure_dev(c, (void **)&c->d_out, &c->out_cap, sizeof(double) * 16));
   k_fold_partials<<<1, 256, 0, c->stream>>>(c->d_partials, nwarps, nsum, c->d_out);
+  c->launches += 1;
   HM_CUDA(c, cudaGetLastError());
   HM_TRY(ensure_host(c, (void **)&c->h_out, &c->h_out_cap, sizeof(double) * 16 + 64));
   HM_CUDA(c, cudaMemcpyAsync(c->h_out, c->d_out, sizeof(double) * 2 * nsum, cudaMemcpyDeviceToHost, c->stream));
-  unsigned *h_err = (unsigned *)(c->h_out + 14);
-  *h_err = 0;
-  const bool twopass = (n - 1) > 10;
-  if (twopass) {
-    HM_CUDA(c, cudaMemcpyAsync(h_err, c->d_ctrl + 2, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
-    HM_CUDA(c, cudaMemcpyAsync(c->h_out + 12, c->d_ctrl + 4 + 2 * twopass_cfg().S, 2 * sizeof(unsigned long long),
-                               cudaMemcpyDeviceToHost, c->stream));
-  }
   HM_CUDA(c, cudaStreamSynchronize(c->stream));
   float ms = 0.f;
   HM_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
   c->last_ms = ms;
-  if (twopass) {
-    const unsigned long long *st = reinterpret_cast<const unsigned long long *>(c->h_out + 12);
-    c->last_wait_frac = st[1] ? (double)st[0] / (double)st[1] : 0.0;
-  }
-  if (twopass && *h_err)
-    return set_err(c, HM_ERR_TIMEOUT, "two-pass sweep: a dependency wait exceeded its limit; results invalid");
   out_dd[0] = c->h_out[0];
   out_dd[1] = c->h_out[1];
   for (int i = 0; i < q.nq; ++i) {
     out_dd[2 + 2 * i] = c->h_out[2 * idx[i]];
     out_dd[3 + 2 * i] = c->h_out[2 * idx[i] + 1];
   }
-  if (twopass && kb == 0) {
+  if (split_zero) {
     // x = 0 (F = WHT of |psi|^2) is not part of the two-pass sweep: one FP64 transform
     // through the plain path, added as a double-double term
     const double ms_main = c->last_ms;
@@ -164,48 +163,35 @@ int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, 
 
 }  // namespace hm
 
-// fraction of CTA time spent in dependency waits during the last two-pass sweep
-extern "C" int hm_debug_wait_fraction(hm_ctx *c, double *out) {
-  if (!c || !out) return HM_ERR_ARG;
-  *out = c->last_wait_frac;
-  return HM_OK;
-}
-
 extern "C" int hm_set_param(int param, int value) {
   hm::TwoPassCfg &cfg = hm::twopass_cfg();
-  if (param == HM_PARAM_BATCH) {
-    if (value == 0) {
-      cfg.X_set = 0;
+  const hm::TwoPassCfg def;
+  switch (param) {
+    case HM_PARAM_BATCH:
+      if (value == 0) {
+        cfg.X_set = 0;
+        return HM_OK;
+      }
+      if (value < 1 || value > 4096 || (value & (value - 1))) return HM_ERR_ARG;
+      cfg.X = value;
+      cfg.X_set = 1;
       return HM_OK;
-    }
-    if (value < 2 || value > 64 || (value & (value - 1))) return HM_ERR_ARG;
-    cfg.X = value;
-    cfg.X_set = 1;
-    return HM_OK;
+    case HM_PARAM_UNITS:
+      if (value == 0) value = def.units_target;
+      if (value < 256 || value > (1 << 20)) return HM_ERR_ARG;
+      cfg.units_target = value;
+      return HM_OK;
+    case HM_PARAM_RING:
+      if (value == 0) value = def.ring_mib;
+      if (value < 8 || value > 4096) return HM_ERR_ARG;
+      cfg.ring_mib = value;
+      return HM_OK;
+    case HM_PARAM_GRAPH:
+      if (value == 0) value = def.graph_stages;
+      if (value < 1 || value > 1024) return HM_ERR_ARG;
+      cfg.graph_stages = value;
+      return HM_OK;
+    default:
+      return HM_ERR_ARG;
   }
-  if (param == 106) {  // pass-1 partner row through shared memory (experiments)
-    cfg.stage_b = value;
-    return HM_OK;
-  }
-  if (param == 105) {  // completion-signal flavour (experiments)
-    cfg.release = value;
-    return HM_OK;
-  }
-  if (param == 104) {  // per-lane fences on/off (experiments)
-    cfg.fence_all = value ? 1 : 0;
-    return HM_OK;
-  }
-  if (param == HM_PARAM_UNITS) {
-    if (value == 0) value = hm::TwoPassCfg().upw;
-    if (value < 1 || value > 64 || (value & (value - 1))) return HM_ERR_ARG;
-    cfg.upw = value;
-    return HM_OK;
-  }
-  if (param == HM_PARAM_RING) {
-    if (value == 0) value = hm::TwoPassCfg().S;
-    if (value < 2 || value > 8) return HM_ERR_ARG;
-    cfg.S = value;
-    return HM_OK;
-  }
-  return HM_ERR_ARG;
 }

@@ -6,17 +6,16 @@
 
 namespace hm {
 
-// Tunables of the two-pass sweep: X-strings per batch and ring slots.  X * S * 2^(n-1)
-// complex values are live in the ring; at n = 20 (FP64) X = 2, S = 3 is 48 MiB, which
-// stays resident in the 126 MB L2 next to the 16 MiB state.
+// Tunables of the two-pass stage kernels (the autotuner sets them through hm_set_param):
+// a batch holds about `units_target` warp units per pass (X = units_target / 2^HI
+// X-strings, or X when set explicitly), the two-batch ring stays within `ring_mib`
+// (L2 resident), and `graph_stages` stages are captured per CUDA graph.
 struct TwoPassCfg {
-  int X = 2;
-  int X_set = 0;  // X was set explicitly (otherwise 2 for FP64, 4 for FP32)
-  int S = 3;
-  int upw = 1;  // warp units per warp per CTA item
-  int fence_all = 0;  // every lane fences its own stores before the completion signal
-  int release = 0;    // completion signal: 0 fence.sc + atomic, 1 red.release, 2 fence.acq_rel + atomic
-  int stage_b = 0;    // pass 1 stages the partner row through shared memory (cp.async)
+  int X = 0;
+  int X_set = 0;
+  int units_target = 4096;
+  int ring_mib = 64;
+  int graph_stages = 32;
 };
 
 TwoPassCfg &twopass_cfg();
@@ -43,59 +42,81 @@ static int launch_fused(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
                     sizeof(double) * 2 * (QSet<QS>::NQ + 1) * (size_t)nwarps));
   a.partials = c->d_partials;
   kern<<<(unsigned)blocks, FUSED_WARPS * 32, smem, c->stream>>>(a);
+  c->launches += 1;
   HM_CUDA(c, cudaGetLastError());
   *nwarps_out = nwarps;
   return HM_OK;
 }
 
+// Stage-kernel two-pass sweep (see k_sre_stage): X-strings per batch sized so that a
+// pass holds about `units_target` warp units, ring of two batches, stages replayed from
+// a captured CUDA graph.
 template <typename T, int R, int HI, int QS>
-static int launch_2pass(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
+static int launch_stages(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
   using V = typename VT<T>::V;
-  SreArgs a = a0;
   const TwoPassCfg cfg = twopass_cfg();
+  constexpr int PB = ilog2c(R) + 5, NQ = QSet<QS>::NQ;
+  StageArgs a;
+  memset(&a, 0, sizeof a);
+  a.psi = a0.psi;
+  a.k_begin = a0.k_begin;
+  a.k_end = a0.k_end;
+  a.qp = a0.qp;
+  a.n = a0.n;
+  const uint64_t U = 1ull << HI;
+  const uint64_t len = a.k_end - a.k_begin;
+  uint64_t X = cfg.X_set ? (uint64_t)cfg.X : std::max<uint64_t>(1, (uint64_t)cfg.units_target / U);
+  // ring bytes 2 X 2^(n-1) sizeof(V) within the budget
+  const uint64_t per_x = ((uint64_t)1 << (a.n - 1)) * sizeof(V);
+  while (X > 1 && 2 * X * per_x > ((uint64_t)cfg.ring_mib << 20)) X >>= 1;
+  if (X > len) X = len;
+  a.X = (int)X;
+  a.nbatch = (int)((len + X - 1) / X);
+  const size_t ring_bytes = 2 * (size_t)X * per_x;
+  HM_TRY(ensure_dev(c, &c->d_inter, &c->inter_cap, ring_bytes));
+  a.ring = c->d_inter;
+  if (a.k_begin < (1ull << PB)) {
+    const size_t slen = (size_t)1 << a.n;
+    HM_TRY(ensure_dev(c, &c->d_aux2, &c->aux2_cap, (size_t)PB * slen * sizeof(V)));
+    k_psi_swapped<V><<<c->num_sms * 8, 256, 0, c->stream>>>(reinterpret_cast<const V *>(a.psi),
+                                                            reinterpret_cast<V *>(c->d_aux2), a.n, PB);
+    c->launches += 1;
+    HM_CUDA(c, cudaGetLastError());
+    for (int j = 0; j < PB; ++j) a.psi_sw[j] = reinterpret_cast<const V *>(c->d_aux2) + (size_t)j * slen;
+  }
   const size_t smem = (size_t)SRE_WARPS * 32 * R * sizeof(V);
-  auto kern = k_sre_2pass<T, R, HI, QS>;
+  auto kern = k_sre_stage<T, R, HI, QS>;
   HM_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int occ = 0;
   HM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, SRE_WARPS * 32, smem));
   if (occ < 1) occ = 1;
-  // FP32 rows are half the bytes: twice the X-strings per batch fit the same L2 budget
-  a.X = cfg.X_set ? cfg.X : (sizeof(T) == 8 ? 2 : 4);
-  a.S = cfg.S;
-  a.flags = (cfg.fence_all ? 2 : 0) | (cfg.release == 1 ? 4 : 0) | (cfg.release == 2 ? 8 : 0) | (cfg.stage_b ? 16 : 0);
-  const uint64_t len = a.k_end - a.k_begin;
-  a.nbatch = (int)((len + a.X - 1) / a.X);
-  const uint64_t U = 1ull << HI;
-  a.upw = cfg.upw;
-  while (a.upw > 1 && (uint64_t)a.X * U < (uint64_t)SRE_WARPS * a.upw) a.upw >>= 1;
-  const long long K = (long long)((a.X * U) / (SRE_WARPS * a.upw));  // CTA items per pass per batch
-  a.nitems = 2 * K * (long long)a.nbatch;
-  const size_t inter_bytes = (size_t)a.S * a.X * ((size_t)1 << (a.n - 1)) * sizeof(V);
-  HM_TRY(ensure_dev(c, &c->d_inter, &c->inter_cap, inter_bytes));
-  a.inter = c->d_inter;
-  const size_t ctrl_words = 8 + 2 * (size_t)a.S;
-  HM_TRY(ensure_dev(c, (void **)&c->d_ctrl, &c->ctrl_cap, ctrl_words * sizeof(unsigned)));
-  HM_CUDA(c, cudaMemsetAsync(c->d_ctrl, 0, ctrl_words * sizeof(unsigned), c->stream));
-  a.ctrl = c->d_ctrl;
-  // bit-swapped copies of psi for the X-strings 1 <= x < 2^PB (Gray indices below 2^PB)
-  constexpr int PB = ilog2c(R) + 5;
-  if (a.k_begin < (1ull << PB)) {
-    const size_t len = (size_t)1 << a.n;
-    HM_TRY(ensure_dev(c, &c->d_aux2, &c->aux2_cap, (size_t)PB * len * sizeof(V)));
-    k_psi_swapped<V><<<c->num_sms * 8, 256, 0, c->stream>>>(reinterpret_cast<const V *>(a.psi),
-                                                            reinterpret_cast<V *>(c->d_aux2), a.n, PB);
-    HM_CUDA(c, cudaGetLastError());
-    for (int j = 0; j < PB; ++j) a.psi_sw[j] = reinterpret_cast<const V *>(c->d_aux2) + (size_t)j * len;
-  }
+  long long units = 2 * (long long)X * (long long)U;
   int blocks = c->num_sms * occ;
-  if ((long long)blocks > a.nitems) blocks = (int)a.nitems;
-  if (blocks < 1) blocks = 1;
+  if ((long long)blocks * SRE_WARPS > units) blocks = (int)((units + SRE_WARPS - 1) / SRE_WARPS);
   const int nwarps = blocks * SRE_WARPS;
-  HM_TRY(ensure_dev(c, (void **)&c->d_partials, &c->partials_cap,
-                    sizeof(double) * 2 * (QSet<QS>::NQ + 1) * (size_t)nwarps));
-  a.partials = c->d_partials;
-  kern<<<blocks, SRE_WARPS * 32, smem, c->stream>>>(a);
-  HM_CUDA(c, cudaGetLastError());
+  HM_TRY(ensure_dev(c, (void **)&c->d_partials, &c->partials_cap, sizeof(double) * 2 * (NQ + 1) * (size_t)nwarps));
+  HM_CUDA(c, cudaMemsetAsync(c->d_partials, 0, sizeof(double) * 2 * (NQ + 1) * (size_t)nwarps, c->stream));
+  a.slots = c->d_partials;
+  HM_TRY(ensure_dev(c, (void **)&c->d_ctrl, &c->ctrl_cap, 4 * sizeof(unsigned)));
+  HM_CUDA(c, cudaMemsetAsync(c->d_ctrl, 0, 4 * sizeof(unsigned), c->stream));
+  a.stage = c->d_ctrl;
+  const int nst = a.nbatch + 1;
+  const int G = std::min(nst, cfg.graph_stages);
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  HM_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  for (int s = 0; s < G; ++s) kern<<<blocks, SRE_WARPS * 32, smem, c->stream>>>(a);
+  cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
+  if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "stage graph capture failed: %s", cudaGetErrorString(ce));
+  ce = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "stage graph instantiation failed: %s", cudaGetErrorString(ce));
+  for (int s = 0; s < nst && ce == cudaSuccess; s += G) {
+    ce = cudaGraphLaunch(exec, c->stream);
+    c->launches += G;
+  }
+  cudaGraphExecDestroy(exec);
+  if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "stage graph launch failed: %s", cudaGetErrorString(ce));
   *nwarps_out = nwarps;
   return HM_OK;
 }
@@ -105,7 +126,7 @@ static int launch_2pass(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
     return launch_fused<T, R, ((NBv) <= PB ? (NBv) : PB), QS>(c, a, nw);
 #define HM_2P_CASE(HIv)                                            \
   case HIv:                                                        \
-    return launch_2pass<T, R, ((HIv) <= PB ? (HIv) : PB), QS>(c, a, nw);
+    return launch_stages<T, R, ((HIv) <= PB ? (HIv) : PB), QS>(c, a, nw);
 
 template <typename T, int R, int QS>
 static int dispatch_sre(hm_ctx *c, const SreArgs &a, int *nw) {
@@ -159,7 +180,6 @@ int launch_sre_qs(hm_ctx *c, const void *psi_dev, int n, uint64_t kb, uint64_t k
   a.k_begin = kb;
   a.k_end = ke;
   a.qp = qp;
-  a.spin_limit = 1ll << 34;
   return dispatch_sre<T, R, QS>(c, a, nwarps);
 }
 

@@ -65,15 +65,26 @@ const char *hm_last_error(hm_ctx *ctx);
  * stream).  Lets a caller time the kernels with events on that stream. */
 int hm_set_stream(hm_ctx *ctx, void *cuda_stream);
 
-/* Tuning knobs of the exact-SRE sweeps (the autotuner sets them; defaults are used
- * otherwise).  HM_PARAM_BATCH: X-strings per batch of the two-pass sweep (power of two,
- * 2..64); HM_PARAM_RING: batches in flight in the L2 ring (2..8); HM_PARAM_UNITS:
- * row/tile units each warp processes per work item (power of two, 1..64).  Value 0
- * restores the default.  Process-wide. */
+/* Tuning knobs of the exact-SRE two-pass sweep (n >= 12); the autotuner sets them,
+ * defaults apply otherwise.  HM_PARAM_BATCH: X-strings per batch (power of two,
+ * 1..4096; 0 = derive it from HM_PARAM_UNITS); HM_PARAM_RING: budget of the two-batch
+ * intermediate ring in MiB (8..4096; it should stay L2 resident); HM_PARAM_UNITS: warp
+ * units per pass the automatic batch size aims for (256..2^20); HM_PARAM_GRAPH: stage
+ * kernels captured per CUDA graph (1..1024).  Value 0 restores the default.
+ * Process-wide; returns HM_ERR_ARG for an unknown knob or value. */
 #define HM_PARAM_BATCH 1
 #define HM_PARAM_RING 2
 #define HM_PARAM_UNITS 3
+#define HM_PARAM_GRAPH 4
 int hm_set_param(int param, int value);
+
+/* Number of kernels the last call launched on the device (graph nodes included). */
+int hm_last_launch_count(hm_ctx *ctx, long long *count);
+
+/* Measured FP64 add throughput of the device, in operations per second (a register-
+ * resident DADD kernel of about 10 ms).  Measurement utility for roofline reports; no
+ * reference counterpart. */
+int hm_probe_fp64_peak(hm_ctx *ctx, double *ops_per_s);
 
 /* Device time in milliseconds of the main kernels of the last call (CUDA events on the
  * context's stream, recorded around the launches that do the transform work). */

@@ -1,0 +1,124 @@
+"""Exact SRE on the GPU against the oracle.  Tolerances: FP64 and the plain path
+1e-10 relative (the stated FP64 bound; observed ~1e-15); FP32 butterflies 1e-6
+relative (observed ~1e-9), plus 1e-9 absolute for values near zero.  Full-size (n = 20) cases use size-independent properties:
+analytic values of product and stabilizer states, Parseval (lost_norm), and Gray
+sub-ranges checked against the oracle."""
+import numpy as np
+import pytest
+
+from conftest import ghz, rand_state, t_state
+
+pytestmark = pytest.mark.gpu
+
+TOL = {"fp64": 1e-10, "plain": 1e-10, "fp32": 1e-6}
+
+
+@pytest.mark.parametrize("n", list(range(1, 17)))
+def test_sre_matches_oracle(ctx, hm, oracle, n):
+    psi = rand_state(1 << n, 100 + n)
+    ref2, lost = oracle.sre(psi, 2)
+    ref3, _ = oracle.sre(psi, 3)
+    for prec in ("fp64", "fp32", "plain"):
+        v, l = ctx.sre(psi, (2.0, 3.0), hm.PRECISIONS[prec])
+        assert v[0] == pytest.approx(ref2, rel=TOL[prec]), prec
+        assert v[1] == pytest.approx(ref3, rel=TOL[prec]), prec
+        assert l < (1e-12 if prec != "fp32" else 1e-6)
+
+
+@pytest.mark.parametrize("q", [1.0, 2.5, 4.0])
+def test_generic_q(ctx, hm, oracle, q):
+    for n in (5, 13):
+        psi = rand_state(1 << n, 7 * n)
+        ref, _ = oracle.sre(psi, q)
+        v, _ = ctx.sre(psi, (q,), hm.HM_FP64)
+        assert v[0] == pytest.approx(ref, rel=1e-10)
+
+
+def test_public_api_matches_reference_semantics(hm, oracle, golden):
+    for g in golden["sre"]:
+        n, q = g["n"], g["q"]
+        psi = (np.array(g["re"]) + 1j * np.array(g["im"])) if g["kind"] == "random" else (
+            t_state(n) if g["kind"] == "t_state" else ghz(n))
+        v, lost = hm.SRE(hm.StateVec(psi), q)
+        assert v == pytest.approx(g["sre"], rel=1e-10, abs=1e-12)
+        assert lost < 1e-12
+
+
+@pytest.mark.parametrize("n", [18, 20])
+def test_full_size_known_answers(ctx, hm, n):
+    for prec in ("fp64", "fp32"):
+        tol = TOL[prec]
+        v, l = ctx.sre(t_state(n), (2.0, 3.0), hm.PRECISIONS[prec])
+        assert v[0] == pytest.approx(n * np.log2(4 / 3), rel=tol)
+        assert v[1] == pytest.approx(n * np.log2(8 / 5), rel=tol)
+        v, l = ctx.sre(ghz(n), (2.0,), hm.PRECISIONS[prec])
+        assert abs(v[0]) < 10 * tol
+        v, l = ctx.sre(rand_state(1 << n, n), (2.0,), hm.PRECISIONS[prec])
+        assert l < (1e-12 if prec == "fp64" else 1e-6)
+
+
+@pytest.mark.parametrize("n", [17, 20])
+def test_gray_subranges_match_oracle(ctx, hm, oracle, n):
+    psi = rand_state(1 << n, n + 1)
+    N = 1 << n
+    for kb, ke in [(0, 24), (1000, 1030), (N // 2 + 5, N // 2 + 40), (N - 21, N)]:
+        p2r, mr = oracle.sre_sums(psi, 2, kb + 1, ke)
+        p2, m = ctx.sre_range(psi, kb, ke, (2.0,), hm.HM_FP64)
+        assert p2.sum() == pytest.approx(p2r, rel=1e-12)
+        assert m.sum() == pytest.approx(mr, rel=1e-12)
+
+
+def test_range_additivity_and_determinism(ctx, hm):
+    n = 15
+    psi = rand_state(1 << n, 3)
+    full_p2, full_m = ctx.sre_range(psi, 0, 1 << n, (2.0,), hm.HM_FP64)
+    a = ctx.sre_range(psi, 0, 12345, (2.0,), hm.HM_FP64)
+    b = ctx.sre_range(psi, 12345, 1 << n, (2.0,), hm.HM_FP64)
+    s = hm.shard.dd_fold([a[1][0], b[1][0]])
+    assert s[0] + s[1] == pytest.approx(full_m.sum(), rel=1e-15)
+    again = ctx.sre_range(psi, 0, 1 << n, (2.0,), hm.HM_FP64)
+    assert np.array_equal(again[1], full_m) and np.array_equal(again[0], full_p2)
+
+
+def test_device_pointer_entry(ctx, hm, oracle):
+    import torch
+    n = 14
+    psi = rand_state(1 << n, 5)
+    t = torch.from_numpy(psi.view(np.float64).copy()).cuda()
+    v, l = ctx.sre_dev(t.data_ptr(), n, (2.0,), hm.HM_FP64)
+    assert v[0] == pytest.approx(oracle.sre(psi, 2)[0], rel=1e-10)
+    with pytest.raises(hm.ArgumentError):
+        ctx.sre_dev(t.data_ptr() + 8, n, (2.0,), hm.HM_FP64)  # not 16-byte aligned
+
+
+def test_argument_errors(ctx, hm):
+    with pytest.raises(hm.ArgumentError):
+        ctx.sre(rand_state(8, 1), (0.5,), hm.HM_FP64)
+    with pytest.raises(hm.ArgumentError):
+        ctx.sre(rand_state(8, 1), (2.0,), 7)
+    with pytest.raises(hm.ArgumentError):
+        ctx.sre_range(rand_state(8, 1), 5, 9, (2.0,), hm.HM_FP64)
+    with pytest.raises(hm.ArgumentError):
+        ctx.sre(rand_state(8, 1), (2.0, 3.0, 2.0, 3.0, 2.0), hm.HM_FP64)
+
+
+def test_gray_tables_bit_exact(ctx, oracle):
+    for n in list(range(0, 13)) + [20]:
+        c, f = ctx.gray_table(n)
+        co, fo = oracle.gray_binary(n)
+        assert np.array_equal(c, co) and np.array_equal(f, fo)
+    for n, q in [(2, 3), (1, 4), (6, 3), (10, 3), (4, 5)]:
+        x, f = ctx.gray_table_general(n, q)
+        xo, fo = oracle.gray_general(n, q)
+        assert np.array_equal(x, xo) and np.array_equal(f, fo)
+
+
+def test_batched_matches_per_state(ctx, hm, oracle):
+    rng = np.random.default_rng(512)
+    ns = [int(v) for v in rng.integers(1, 16, size=24)]
+    psis = [rand_state(1 << n, 10_000 + i) for i, n in enumerate(ns)]
+    for prec in ("fp64", "fp32"):
+        vals, lost = ctx.sre_batched(psis, (2.0, 3.0), hm.PRECISIONS[prec])
+        for i, p in enumerate(psis):
+            assert vals[i, 0] == pytest.approx(oracle.sre(p, 2)[0], rel=TOL[prec], abs=1e-9)
+            assert vals[i, 1] == pytest.approx(oracle.sre(p, 3)[0], rel=TOL[prec], abs=1e-9)
