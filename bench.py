@@ -107,7 +107,7 @@ class ClockSampler:
 
 
 def cpu_baseline(n, seconds=12.0):
-    """The oracle (C restatement of src/Backends/Threads.jl:263-314, OpenMP static
+    """The oracle (C restatement of src/Backends/Threads.jl:108-159, OpenMP static
     partition) on a sample of Gray indices; returns Pauli strings / s."""
     from oracle import oracle as O
     O.build()

@@ -163,7 +163,7 @@ def SRE(psi, q, backend="auto", progress=False, precision="fp64", device=0):
 
     value = -log2(sum_P <psi|P|psi>^(2q) / 2^n) over all 4^n Pauli strings and
     lost_norm = |1 - sum_P <psi|P|psi>^2 / 2^n|, as src/SRE.jl:75-83 and
-    src/Backends/Threads.jl:263-314 (for q != 2 the value is (q-1) M_q, as there).
+    src/Backends/Threads.jl:108-159 (for q != 2 the value is (q-1) M_q, as there).
     precision: "fp64" (default), "fp32" (FP32 butterflies, FP64 reductions) or "plain"
     (the reference CUDA backend's multi-launch structure, FP64).
     """
@@ -215,7 +215,7 @@ def proposal_stream(L, Nbeta, Nsamples, seed=None):
 
 def MC_SRE(psi, q, backend="auto", Nbeta=13, Nsamples=1000, seed=None, progress=False, device=0,
            prop_delta=None, rs=None):
-    """Monte-Carlo SRE_q (src/SRE.jl:33-43, src/Backends/Threads.jl:316-376).
+    """Monte-Carlo SRE_q (src/SRE.jl:33-43, src/Backends/Threads.jl:161-221).
 
     Nbeta chains at beta_i = (i-1)/(Nbeta-1) (Nbeta odd, Simpson's rule); returns
     -log2(2^-I + I_add).  The proposal stream comes from proposal_stream(seed) unless
@@ -236,7 +236,7 @@ def Mana(psi, backend="auto", progress=False, device=0):
     """Mana of a qutrit state.
 
     StateVec (q=3): log2(sum |W|) / log2(3) over the phase-space transforms of every
-    ternary X-string (src/Mana.jl:15-92, src/Backends/Threads.jl:378-426).
+    ternary X-string (src/Mana.jl:15-92, src/Backends/Threads.jl:223-271).
     DensityMatrix (q=3): log2(sum |M^(x)N vec9(rho)| / 3^N) (src/Mana.jl:305-314).
     """
     _progress_warning(progress)
@@ -250,7 +250,7 @@ def Mana(psi, backend="auto", progress=False, device=0):
 
 
 def generate_gray_table(n, q):
-    """Gray table as src/Basis.jl:544-557, computed on the device.
+    """Gray table as src/Basis.jl:252-265, computed on the device.
 
     q == 2: (codes uint64[2^n], flips int64[2^n - 1], 1-based).
     q > 2:  (XTAB int64[n, q^n], flips int64[q^n - 1], 1-based).

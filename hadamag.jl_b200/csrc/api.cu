@@ -59,7 +59,7 @@ __global__ void k_gray_binary(uint64_t *codes, int64_t *flips, uint64_t N) {
   }
 }
 
-// integer_to_gray (src/Basis.jl:415-425): base-q digits least significant first, folded
+// integer_to_gray (src/Basis.jl:123-133): base-q digits least significant first, folded
 // from the most significant digit down with a running shift.
 __device__ void q_gray(uint64_t val, int q, int n, int64_t *out) {
   int64_t shift = 0;

@@ -1,6 +1,6 @@
 // mana.cu -- qutrit Mana kernels.
 //
-// Pure states (src/Mana.jl:19-92, src/Backends/Threads.jl:378-426).  For every ternary
+// Pure states (src/Mana.jl:19-92, src/Backends/Threads.jl:223-271).  For every ternary
 // X-string x the reference forms
 //     v(r) = conj psi(r (+) x) * (psi((-r) (+) x) / 3^L)        ((+): digitwise addition mod 3)
 // applies the qutrit Hadamard H3^{(x)L} (src/Helpers.jl:249-292) and sums |W|; the Mana

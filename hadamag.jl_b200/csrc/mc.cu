@@ -1,5 +1,5 @@
 // mc.cu -- MC_SRE: Metropolis chains over X-strings (src/SRE.jl:110-192,
-// src/Backends/Threads.jl:316-376, Simpson of src/Helpers.jl:223-236).
+// src/Backends/Threads.jl:161-221, Simpson of src/Helpers.jl:223-236).
 //
 // All Nbeta chains advance together.  One step is: evaluate m(x) and p2(x) of every
 // chain's proposal with the warp engine of the exact-SRE sweep (one warp per chain for

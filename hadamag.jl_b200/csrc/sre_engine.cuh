@@ -113,9 +113,7 @@ __device__ __forceinline__ double pow_q_dev(double y, double q) {
 }
 
 // Per-lane sums of F^2 and of (F^2)^q over the R complex registers (2R values of F/2
-// for x != 0; the caller applies the 4 / 4^q scale).  FP64: plain sums in a fixed
-// order.  FP32: eight interleaved float accumulators per sum, combined pairwise, then
-// promoted to double.
+// for x != 0; the caller applies the 4 / 4^q scale), plain FP64 sums in a fixed order.
 // Generic Renyi indices: the F values go through the warp's shared buffer so that the
 // pow() evaluations run in a rolled loop instead of an unrolled register sweep.
 template <int R, typename V>
@@ -138,9 +136,10 @@ __device__ __noinline__ void lane_moments_gen(const V *sm, int lane, double *s, 
   for (int t = 0; t < 4; ++t) s[1 + t] = ag[t];
 }
 
-template <int R, int QS>
-__device__ __forceinline__ void lane_moments(const double2 (&v)[R], double *s, const QParams &qp, double2 *sm,
-                                             int lane) {
+// Both precisions take the powers and the sums in FP64: an FP32 value of F converts to
+// double exactly, so the FP32 path's only roundings are those of f and of the butterflies.
+template <int R, int QS, typename V>
+__device__ __forceinline__ void lane_moments(const V (&v)[R], double *s, const QParams &qp, V *sm, int lane) {
   if constexpr (QS == QS_GEN) {
 #pragma unroll
     for (int i = 0; i < R; ++i) sm[lane + 32 * i] = v[i];
@@ -153,7 +152,7 @@ __device__ __forceinline__ void lane_moments(const double2 (&v)[R], double *s, c
     for (int i = 0; i < R; ++i) {
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
-        const double f = c ? v[i].y : v[i].x;
+        const double f = c ? (double)v[i].y : (double)v[i].x;
         const double y = f * f;
         a2 += y;
         a4 = fma(y, y, a4);
@@ -163,46 +162,6 @@ __device__ __forceinline__ void lane_moments(const double2 (&v)[R], double *s, c
     s[0] = a2;
     s[1] = a4;
     if constexpr (QS == QS_Q23) s[2] = a6;
-  }
-}
-
-template <int R, int QS>
-__device__ __forceinline__ void lane_moments(const float2 (&v)[R], double *s, const QParams &qp, float2 *sm,
-                                             int lane) {
-  if constexpr (QS == QS_GEN) {
-#pragma unroll
-    for (int i = 0; i < R; ++i) sm[lane + 32 * i] = v[i];
-    lane_moments_gen<R>(sm, lane, s, qp);
-    __syncwarp();
-    return;
-  } else {
-    constexpr int NA = 8;
-    float a2[NA], a4[NA], a6[NA];
-#pragma unroll
-    for (int t = 0; t < NA; ++t) a2[t] = a4[t] = a6[t] = 0.f;
-#pragma unroll
-    for (int i = 0; i < R; ++i) {
-#pragma unroll
-      for (int c = 0; c < 2; ++c) {
-        const float f = c ? v[i].y : v[i].x;
-        const float y = f * f;
-        const int t = (2 * i + c) % NA;
-        a2[t] += y;
-        a4[t] = fmaf(y, y, a4[t]);
-        if constexpr (QS == QS_Q23) a6[t] = fmaf(y * y, y, a6[t]);
-      }
-    }
-#pragma unroll
-    for (int w = NA / 2; w > 0; w >>= 1)
-#pragma unroll
-      for (int t = 0; t < w; ++t) {
-        a2[t] += a2[t + w];
-        a4[t] += a4[t + w];
-        a6[t] += a6[t + w];
-      }
-    s[0] = (double)a2[0];
-    s[1] = (double)a4[0];
-    if constexpr (QS == QS_Q23) s[2] = (double)a6[0];
   }
 }
 

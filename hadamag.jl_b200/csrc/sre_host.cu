@@ -107,8 +107,10 @@ int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, 
   const int kind = choose_qs(q, qp, idx);
   const int nsum = 1 + (kind == QS_Q2 ? 1 : (kind == QS_Q23 ? 2 : 4));
   const uint64_t len = 1ull << n;
+  // the fused kernels (n <= 11) read the FP64 state in both precisions; the FP32 two-pass
+  // kernels read an FP32 copy
   const void *psi_k = psi_dev;
-  if (precision == HM_FP32) {
+  if (precision == HM_FP32 && (n - 1) > 10) {
     HM_TRY(ensure_dev(c, &c->d_psi32, &c->psi32_cap, len * sizeof(float2)));
     k_psi_to_f32<<<c->num_sms * 4, 256, 0, c->stream>>>(psi_dev, (float2 *)c->d_psi32, len);
     c->launches += 1;

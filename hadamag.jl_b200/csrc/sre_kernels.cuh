@@ -1,5 +1,5 @@
 // sre_kernels.cuh -- exact-SRE kernels (fused single-warp sweep for n <= PB+1, and the
-// persistent two-pass sweep for larger n) plus the deterministic double-double fold.
+// two-pass stage kernels for larger n) plus the deterministic double-double fold.
 #pragma once
 #include "sre_engine.cuh"
 
@@ -28,6 +28,8 @@ __device__ __forceinline__ void write_partials(double *partials, int gwarp, cons
 // ---------------------------------------------------------------------------------
 // Fused sweep, n - 1 = NB <= PB element bits: one warp holds 2^(PB - NB) X-strings
 // (consecutive Gray indices), builds, transforms and reduces them without leaving the SM.
+// The state is always read in FP64 and f = conj(psi(r)) psi(r ^ x) is formed in FP64;
+// the FP32 variant rounds f, not psi, so that its error stays second order.
 template <typename T, int R, int NB, int QS>
 __global__ void __launch_bounds__(FUSED_WARPS * 32) k_sre_fused(SreArgs a) {
   using V = typename VT<T>::V;
@@ -39,7 +41,7 @@ __global__ void __launch_bounds__(FUSED_WARPS * 32) k_sre_fused(SreArgs a) {
   const int lane = threadIdx.x & 31;
   const int gwarp = blockIdx.x * FUSED_WARPS + (threadIdx.x >> 5);
   const int nwarps = gridDim.x * FUSED_WARPS;
-  const V *psi = reinterpret_cast<const V *>(a.psi);
+  const double2 *psi = reinterpret_cast<const double2 *>(a.psi);
   constexpr uint64_t XPW = 1ull << (PB - NB);
   const uint64_t ngroups = (a.k_end - a.k_begin + XPW - 1) / XPW;
   dd acc[NQ + 1];
@@ -54,9 +56,7 @@ __global__ void __launch_bounds__(FUSED_WARPS * 32) k_sre_fused(SreArgs a) {
       const uint32_t e = (uint32_t)(i * 32 + lane);
       const uint64_t xl = e >> NB, rp = e & ((1u << NB) - 1u);
       const uint64_t k = kbase + xl;
-      V f;
-      f.x = 0;
-      f.y = 0;
+      double2 f = make_double2(0.0, 0.0);
       if (k < a.k_end) {
         const uint64_t x = gray_code(k);
         if (x == 0) {
@@ -71,7 +71,8 @@ __global__ void __launch_bounds__(FUSED_WARPS * 32) k_sre_fused(SreArgs a) {
           }
         }
       }
-      v[i] = f;
+      v[i].x = (T)f.x;
+      v[i].y = (T)f.y;
     }
     if constexpr (NB > 5) reg_wht<R, 0, NB - 5>(v);
     transpose_ab<R>(v, sm, lane);

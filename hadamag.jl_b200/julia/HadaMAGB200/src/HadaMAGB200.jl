@@ -1,0 +1,139 @@
+"""
+    HadaMAGB200
+
+B200 backend for HadaMAG.jl: exact SRE, MC_SRE and Mana on an NVIDIA B200 through
+libhadamag_b200.so (C ABI declared in include/hadamag_b200.h).
+
+    using HadaMAG, HadaMAGB200
+    SRE(ψ, 2; backend = HadaMAGB200.B200())
+    MC_SRE(ψ, 2; backend = HadaMAGB200.B200(), Nβ = 13, Nsamples = 1000, seed = 123)
+    Mana(ψ3; backend = HadaMAGB200.B200())
+    HadaMAGB200.Mana(ρ)                       # DensityMatrix{ComplexF64,3}
+    HadaMAGB200.SRE_grad(ψ, 2)                # value and dSRE/dψ (no reference counterpart)
+
+Passing the backend object works with the unmodified package: `_choose_backend` gets a
+method for `B200` and `_apply_backend` routes to the functions below (the dispatch of
+src/Backends/Dispatch.jl:12-90).  A `:b200` symbol needs one extra branch in
+`_choose_backend` of HadaMAG itself.
+
+The functions mirror the backend signatures of ext/HadaMAGCUDAExt.jl:1381-1410 (SRE),
+src/Backends/Threads.jl:161-221 (MC_SRE) and 223-271 (Mana).  MC_SRE draws its proposal
+stream with the calls of src/SRE.jl:142-145 and 164-169 (MersenneTwister(seed + i),
+rand(rng, Nsamples) twice, rand(rng, 1:L) per flip) and hands it to the device, so a
+given seed reproduces the chains of the CPU backends.
+"""
+module HadaMAGB200
+
+using HadaMAG
+using Random
+
+const LIB = Ref{String}(joinpath(@__DIR__, "..", "..", "..", "libhadamag_b200.so"))
+const CTX = Ref{Ptr{Cvoid}}(C_NULL)
+
+const HM_FP64 = Cint(0)
+const HM_FP32 = Cint(1)
+const HM_PLAIN = Cint(2)
+
+struct B200 <: HadaMAG.AbstractBackend end
+
+function context()
+    if CTX[] == C_NULL
+        h = Ref{Ptr{Cvoid}}(C_NULL)
+        rc = ccall((:hm_create, LIB[]), Cint, (Ref{Ptr{Cvoid}}, Cint), h, 0)
+        rc == 0 || error("hm_create failed with status $rc (no usable CUDA device?)")
+        CTX[] = h[]
+        atexit(() -> ccall((:hm_destroy, LIB[]), Cint, (Ptr{Cvoid},), CTX[]))
+    end
+    return CTX[]
+end
+
+# HM_ERR_ARG, HM_ERR_SIZE, HM_ERR_Q and HM_ERR_ALIGN are caller errors
+function check(rc, what)
+    rc == 0 && return nothing
+    msg = unsafe_string(ccall((:hm_last_error, LIB[]), Cstring, (Ptr{Cvoid},), context()))
+    rc in (-1, -2, -3, -7) && throw(ArgumentError("$what: $msg"))
+    error("$what failed with status $rc: $msg")
+end
+
+function SRE(ψ, q::Number; progress = false, precision = HM_FP64, kwargs...)
+    progress && @warn "Progress bar not implemented for the B200 backend."
+    v = collect(ComplexF64, data(ψ))
+    out = zeros(Float64, 1)
+    lost = Ref{Float64}(0.0)
+    rc = ccall((:hm_sre, LIB[]), Cint,
+               (Ptr{Cvoid}, Ptr{Float64}, Cint, Ptr{Float64}, Cint, Cint, Ptr{Float64}, Ref{Float64}),
+               context(), reinterpret(Float64, v), qubits(ψ), Float64[q], 1, precision, out, lost)
+    check(rc, "hm_sre")
+    return (out[1], lost[])
+end
+
+function MC_SRE(ψ, q, Nβ::Int, Nsamples::Int; seed::Union{Nothing,Int} = nothing, progress = true)
+    Nβ % 2 == 1 || error("Simpson needs an odd number of β points.")
+    L = qubits(ψ)
+    base_seed = seed === nothing ? rand(1:(10^9)) : seed
+    pd = Vector{UInt64}(undef, Nβ * Nsamples)
+    rs = Vector{Float64}(undef, Nβ * Nsamples)
+    MASK = UInt64(1) .<< (0:(L-1))
+    for i = 1:Nβ
+        rng = MersenneTwister(base_seed + i)
+        tries = floor.(Int, rand(rng, Nsamples) .* 9) .+ 1
+        r = rand(rng, Nsamples)
+        for t = 1:Nsamples
+            Δ = zero(UInt64)
+            for _ = 1:tries[t]
+                Δ ⊻= MASK[rand(rng, 1:L)]
+            end
+            pd[(i-1)*Nsamples+t] = Δ
+            rs[(i-1)*Nsamples+t] = r[t]
+        end
+    end
+    v = collect(ComplexF64, data(ψ))
+    m2 = Ref{Float64}(0.0)
+    M2, M2ADD, P2 = zeros(Nβ), zeros(Nβ), zeros(Nβ)
+    rc = ccall((:hm_mc_sre, LIB[]), Cint,
+               (Ptr{Cvoid}, Ptr{Float64}, Cint, Cdouble, Cint, Cint, Ptr{UInt64}, Ptr{Float64},
+                Ref{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{Float64}, Ptr{UInt64}),
+               context(), reinterpret(Float64, v), L, Float64(q), Nβ, Nsamples, pd, rs, m2, M2, M2ADD, P2,
+               C_NULL)
+    check(rc, "hm_mc_sre")
+    return m2[]
+end
+
+function Mana(ψ::StateVec{T,3}; progress = false) where {T}
+    v = collect(ComplexF64, data(ψ))
+    out = Ref{Float64}(0.0)
+    rc = ccall((:hm_mana_pure, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Float64}, Cint, Ref{Float64}),
+               context(), reinterpret(Float64, v), qudits(ψ), out)
+    check(rc, "hm_mana_pure")
+    return out[]
+end
+
+function Mana(ρ::DensityMatrix{T,3}; kwargs...) where {T}
+    m = collect(ComplexF64, data(ρ))          # column-major, as Julia stores it
+    out = Ref{Float64}(0.0)
+    rc = ccall((:hm_mana_mixed, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Float64}, Cint, Ref{Float64}),
+               context(), reinterpret(Float64, vec(m)), qudits(ρ), out)
+    check(rc, "hm_mana_mixed")
+    return out[]
+end
+
+"""
+    SRE_grad(ψ, q = 2) -> (value, grad)
+
+Value and gradient of SRE_q; `grad[r] = ∂SRE/∂Re ψ[r] + im * ∂SRE/∂Im ψ[r]`.
+"""
+function SRE_grad(ψ, q = 2)
+    v = collect(ComplexF64, data(ψ))
+    g = similar(v)
+    val = Ref{Float64}(0.0)
+    rc = ccall((:hm_sre_grad, LIB[]), Cint,
+               (Ptr{Cvoid}, Ptr{Float64}, Cint, Cdouble, Ref{Float64}, Ptr{Float64}),
+               context(), reinterpret(Float64, v), qubits(ψ), Float64(q), val, reinterpret(Float64, g))
+    check(rc, "hm_sre_grad")
+    return (val[], g)
+end
+
+HadaMAG._choose_backend(b::B200) = b
+HadaMAG._apply_backend(::B200, fsym, args...; kw...) = getfield(HadaMAGB200, fsym)(args...; kw...)
+
+end # module

@@ -55,7 +55,7 @@ def dd_fold(parts):
 def combine_partials(gathered, n, nq):
     """gathered: array (world, 2 + 2 nq) of [p2_hi, p2_lo, m_hi, m_lo, ...] per rank.
 
-    Returns (sre[nq], lost_norm) as src/Backends/Threads.jl:313.
+    Returns (sre[nq], lost_norm) as src/Backends/Threads.jl:158.
     """
     g = np.asarray(gathered, dtype=np.float64).reshape(-1, 2 + 2 * nq)
     dim = float(1 << n)

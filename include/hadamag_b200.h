@@ -38,7 +38,7 @@ extern "C" {
 #define HM_ERR_Q -3       /* unsupported Renyi index q                                */
 #define HM_ERR_CUDA -4    /* a CUDA runtime call failed (message in hm_last_error)    */
 #define HM_ERR_OOM -5     /* device allocation failed                                 */
-#define HM_ERR_TIMEOUT -6 /* a bounded device-side wait gave up; results are invalid  */
+#define HM_ERR_TIMEOUT -6 /* reserved: no current entry point waits on the device     */
 #define HM_ERR_ALIGN -7   /* device pointer not 16-byte aligned                      */
 
 /* precision / algorithm selector for the exact-SRE entry points */
@@ -96,7 +96,7 @@ int hm_last_kernel_ms(hm_ctx *ctx, double *ms);
 
 /* Exact stabilizer Renyi entropy over all 4^n Pauli strings.
  * Replaces SRE(psi, q; backend=:cuda) of ext/HadaMAGCUDAExt.jl:1381-1410 (and the CPU
- * backends src/Backends/Serial.jl:7-51, src/Backends/Threads.jl:263-314): for each q in
+ * backends src/Backends/Serial.jl:7-51, src/Backends/Threads.jl:108-159): for each q in
  * qs[0..nq), out_sre[i] = -log2(m_q / 2^n) with m_q = sum over x, k of (F_x(k)^2)^q, and
  * out_lost[0] = |1 - p2 / 2^n| with p2 = sum F^2.  As in the reference, for q != 2 the
  * value is (q-1) times the textbook M_q.
@@ -139,7 +139,7 @@ int hm_sre_grad(hm_ctx *ctx, const double *psi, int n, double q, double *out_sre
 /* MC_SRE                                                                               */
 /* ---------------------------------------------------------------------------------- */
 
-/* Metropolis estimate of SRE_q (replaces MC_SRE of src/Backends/Threads.jl:316-376 with
+/* Metropolis estimate of SRE_q (replaces MC_SRE of src/Backends/Threads.jl:161-221 with
  * mc_sre_beta! of src/SRE.jl:110-192).  Chain i runs at beta_i = i / (nbeta - 1).  The
  * proposal stream is an input: prop_delta[i*nsamples + t] is the XOR of the site bits the
  * reference draws for step t of chain i (src/SRE.jl:164-170), rs[i*nsamples + t] its
@@ -154,7 +154,7 @@ int hm_mc_sre(hm_ctx *ctx, const double *psi, int n, double q, int nbeta, int ns
 /* ---------------------------------------------------------------------------------- */
 
 /* Mana of a pure L-qutrit state (3^L interleaved complex doubles, host).
- * Replaces Mana(psi::StateVec{T,3}) of src/Backends/Threads.jl:378-426 with
+ * Replaces Mana(psi::StateVec{T,3}) of src/Backends/Threads.jl:223-271 with
  * compute_chunk_mana_qutrits of src/Mana.jl:19-92: log2(sum |W|) / log2(3).  1 <= L <= 12. */
 int hm_mana_pure(hm_ctx *ctx, const double *psi, int L, double *out_mana);
 
@@ -167,12 +167,12 @@ int hm_mana_mixed(hm_ctx *ctx, const double *rho, int N, double *out_mana);
 /* Gray tables (parity checks of the device-side X-string enumeration)                 */
 /* ---------------------------------------------------------------------------------- */
 
-/* Binary Gray table computed on the device, as generate_binary of src/Basis.jl:306-319:
+/* Binary Gray table computed on the device, as generate_binary of src/Basis.jl:14-27:
  * codes[k] = k ^ (k >> 1) (2^n entries), flips[k] = 1-based bit that flips between
  * codes[k] and codes[k+1] (2^n - 1 entries).  0 <= n <= 30. */
 int hm_gray_table(hm_ctx *ctx, int n, uint64_t *codes, int64_t *flips);
 
-/* q-ary Gray table computed on the device, as generate_general of src/Basis.jl:438-456:
+/* q-ary Gray table computed on the device, as generate_general of src/Basis.jl:146-164:
  * xtab is n x q^n column-major (column k = integer_to_gray(k)), flips has q^n - 1
  * 1-based digit positions.  2 <= q <= 16, q^n <= 2^26. */
 int hm_gray_table_general(hm_ctx *ctx, int n, int q, int64_t *xtab, int64_t *flips);

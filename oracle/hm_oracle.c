@@ -36,7 +36,7 @@
 /* Gray codes                                                                 */
 /* ------------------------------------------------------------------------- */
 
-/* src/Basis.jl:306-319 (generate_binary): codes[k] = k ^ (k >> 1) for k = 0..2^n-1,
+/* src/Basis.jl:14-27 (generate_binary): codes[k] = k ^ (k >> 1) for k = 0..2^n-1,
  * flips[k] (k = 0..2^n-2) = 1-based position of the bit that flips between codes[k]
  * and codes[k+1]. */
 int or_gray_binary(int n, uint64_t *codes, int64_t *flips) {
@@ -76,7 +76,7 @@ int or_gray_binary_split(int n, int rank, int P, uint64_t *codes, int64_t *flips
     return OR_OK;
 }
 
-/* src/Basis.jl:415-425 (integer_to_gray): base-q digits of val least-significant
+/* src/Basis.jl:123-133 (integer_to_gray): base-q digits of val least-significant
  * first, padded to n, folded from the most significant digit down with a running
  * shift: gray[i] = (digit[i] + shift) mod q; shift += q - gray[i]. */
 static void integer_to_gray(int64_t val, int q, int n, int64_t *gray) {
@@ -92,7 +92,7 @@ static void integer_to_gray(int64_t val, int q, int n, int64_t *gray) {
     }
 }
 
-/* src/Basis.jl:438-456 (generate_general): XTAB is n x q^n, column-major (column k is
+/* src/Basis.jl:146-164 (generate_general): XTAB is n x q^n, column-major (column k is
  * integer_to_gray(k)), flips[k] = 1-based first digit where columns k and k+1 differ. */
 int or_gray_general(int n, int q, int64_t *xtab, int64_t *flips) {
     if (n < 0 || n > 40 || q < 2) return OR_ERR_ARG;
@@ -229,7 +229,7 @@ static uint64_t flip_and_update_mask(int site, int64_t dim, uint64_t mask, const
 typedef struct {
     int n;
     int64_t dim;
-    double *X1, *X2, *TMP1, *TMP2; /* src/Backends/Threads.jl:270-283 */
+    double *X1, *X2, *TMP1, *TMP2; /* src/Backends/Threads.jl:115-128 */
 } sre_prep;
 
 static int sre_prep_init(sre_prep *s, const double *psi, int n) {
@@ -298,7 +298,7 @@ static void sre_chunk(const sre_prep *s, double q, int64_t istart, int64_t iend,
 }
 
 /* Raw sums (p2SAM, mSAM) over 1-based Gray indices [istart, iend] split over nthreads
- * exactly as src/Backends/Threads.jl:192-257 (threaded_chunk_reduce): static contiguous
+ * exactly as src/Backends/Threads.jl:37-102 (threaded_chunk_reduce): static contiguous
  * partition_counts slices, per-thread compute_chunk_sre, per-thread results summed in
  * thread order. */
 int or_sre_sums(const double *psi, int n, double q, int64_t istart, int64_t iend, int nthreads, double *p2_out,
@@ -336,7 +336,7 @@ int or_sre_sums(const double *psi, int n, double q, int64_t istart, int64_t iend
     return OR_OK;
 }
 
-/* src/Backends/Threads.jl:263-314 (SRE): (-log2(m/dim), |1 - p2/dim|) over all 2^n
+/* src/Backends/Threads.jl:108-159 (SRE): (-log2(m/dim), |1 - p2/dim|) over all 2^n
  * X-strings.  With nthreads == 1 this is src/Backends/Serial.jl:7-51. */
 int or_sre(const double *psi, int n, double q, int nthreads, double *sre, double *lost) {
     double p2, m;
@@ -494,7 +494,7 @@ double or_simpson_uniform(const double *x, const double *y, int npts) {
     return (h / 3.0) * (y[0] + y[npts - 1] + 4.0 * odd + 2.0 * even);
 }
 
-/* src/Backends/Threads.jl:316-376 (MC_SRE): one chain per beta_i = (i-1)/(Nbeta-1),
+/* src/Backends/Threads.jl:161-221 (MC_SRE): one chain per beta_i = (i-1)/(Nbeta-1),
  * Simpson over M2 and M2ADD, m2 = -log2(2^-I + I_add).  prop_delta and rs hold
  * Nbeta consecutive streams of nsamples each. */
 int or_mc_sre(const double *psi, int n, double q, int nbeta, int nsamples, const uint64_t *prop_delta,
@@ -611,7 +611,7 @@ static double mana_chunk(const double *psi, int L, int64_t dim, const int64_t *X
 }
 
 /* Sum of |W| over the 1-based ternary Gray columns [istart, iend], threaded as
- * src/Backends/Threads.jl:378-426 (static partition, thread-ordered sum). */
+ * src/Backends/Threads.jl:223-271 (static partition, thread-ordered sum). */
 int or_mana_sum(const double *psi, int L, int64_t istart, int64_t iend, int nthreads, double *sum_out) {
     if (L < 0 || L > 16 || nthreads < 1) return OR_ERR_ARG;
     int64_t dim = 1;
@@ -620,7 +620,7 @@ int or_mana_sum(const double *psi, int L, int64_t istart, int64_t iend, int nthr
     int64_t *XTAB = malloc(sizeof(int64_t) * (size_t)dim * (L > 0 ? L : 1));
     int64_t *Zwhere = malloc(sizeof(int64_t) * (size_t)dim);
     or_gray_general(L, 3, XTAB, Zwhere);
-    /* src/Backends/Threads.jl:384-397: AA = digitwise negation mod 3 (0-based here) */
+    /* src/Backends/Threads.jl:229-242: AA = digitwise negation mod 3 (0-based here) */
     int64_t *AA = malloc(sizeof(int64_t) * (size_t)dim);
     for (int64_t i = 0; i < dim; i++) {
         int64_t x = i, y = 0, pw = 1;
@@ -658,7 +658,7 @@ int or_mana_sum(const double *psi, int L, int64_t istart, int64_t iend, int nthr
     return OR_OK;
 }
 
-/* src/Backends/Threads.jl:378-426 (Mana): log2(S)/log2(3). */
+/* src/Backends/Threads.jl:223-271 (Mana): log2(S)/log2(3). */
 int or_mana_pure(const double *psi, int L, int nthreads, double *mana) {
     int64_t dim = 1;
     for (int i = 0; i < L; i++) dim *= 3;

@@ -5,8 +5,8 @@ random states, test/SRE_test.jl:48-55, test/Mana_test.jl:1-12) and Julia is not
 available here, so these fixtures come from a second, independent restatement of the
 reference's definitions in plain Python/numpy, written for small sizes only:
 
-  * Gray tables: src/Basis.jl:306-319 (generate_binary), 368-398 (generate_binary_
-    splitted), 415-456 (integer_to_gray, generate_general), src/Helpers.jl:18-23
+  * Gray tables: src/Basis.jl:14-27 (generate_binary), 76-106 (generate_binary_
+    splitted), 123-164 (integer_to_gray, generate_general), src/Helpers.jl:18-23
     (partition_counts);
   * exact SRE by the naive O(8^n) definition, src/SRE.jl:643-749 (expval_pauli_mask,
     naive_SRE), including the reference's value -log2(sum (e^2)^q / 2^n) for q != 2;

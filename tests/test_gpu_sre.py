@@ -1,8 +1,11 @@
 """Exact SRE on the GPU against the oracle.  Tolerances: FP64 and the plain path
-1e-10 relative (the stated FP64 bound; observed ~1e-15); FP32 butterflies 1e-6
-relative (observed ~1e-9), plus 1e-9 absolute for values near zero.  Full-size (n = 20) cases use size-independent properties:
-analytic values of product and stabilizer states, Parseval (lost_norm), and Gray
-sub-ranges checked against the oracle."""
+1e-10 relative (the stated FP64 bound; observed ~1e-15).  FP32 butterflies: 1e-6
+relative or 1e-6 absolute, whichever is larger.  The absolute term covers values below
+one: rounding each product f = conj(psi(r)) psi(r ^ x) to FP32 (2^-24 relative) already
+moves SRE by about 1e-7 in absolute terms, so no relative bound holds as SRE -> 0 (an
+n = 1 state with SRE_2 = 0.067 shows 1.2e-6 relative).  Full-size (n = 20) cases use
+size-independent properties: analytic values of product and stabilizer states,
+Parseval (lost_norm), and Gray sub-ranges checked against the oracle."""
 import numpy as np
 import pytest
 
@@ -11,6 +14,11 @@ from conftest import ghz, rand_state, t_state
 pytestmark = pytest.mark.gpu
 
 TOL = {"fp64": 1e-10, "plain": 1e-10, "fp32": 1e-6}
+ABS = {"fp64": 0.0, "plain": 0.0, "fp32": 1e-6}
+
+
+def close(ref, prec):
+    return pytest.approx(ref, rel=TOL[prec], abs=ABS[prec])
 
 
 @pytest.mark.parametrize("n", list(range(1, 17)))
@@ -20,8 +28,8 @@ def test_sre_matches_oracle(ctx, hm, oracle, n):
     ref3, _ = oracle.sre(psi, 3)
     for prec in ("fp64", "fp32", "plain"):
         v, l = ctx.sre(psi, (2.0, 3.0), hm.PRECISIONS[prec])
-        assert v[0] == pytest.approx(ref2, rel=TOL[prec]), prec
-        assert v[1] == pytest.approx(ref3, rel=TOL[prec]), prec
+        assert v[0] == close(ref2, prec), prec
+        assert v[1] == close(ref3, prec), prec
         assert l < (1e-12 if prec != "fp32" else 1e-6)
 
 
@@ -120,5 +128,5 @@ def test_batched_matches_per_state(ctx, hm, oracle):
     for prec in ("fp64", "fp32"):
         vals, lost = ctx.sre_batched(psis, (2.0, 3.0), hm.PRECISIONS[prec])
         for i, p in enumerate(psis):
-            assert vals[i, 0] == pytest.approx(oracle.sre(p, 2)[0], rel=TOL[prec], abs=1e-9)
-            assert vals[i, 1] == pytest.approx(oracle.sre(p, 3)[0], rel=TOL[prec], abs=1e-9)
+            assert vals[i, 0] == close(oracle.sre(p, 2)[0], prec)
+            assert vals[i, 1] == close(oracle.sre(p, 3)[0], prec)

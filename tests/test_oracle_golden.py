@@ -124,7 +124,7 @@ def test_mana_known_answers(oracle):
         assert abs(oracle.mana_pure(psi)) < 1e-14
         assert abs(oracle.mana_mixed(np.eye(3 ** L) / 3 ** L)) < 1e-13
         psi = rand_state(3 ** L, 5 + L)
-        # the two log bases (src/Backends/Threads.jl:425 vs src/Mana.jl:311)
+        # the two log bases (src/Backends/Threads.jl:270 vs src/Mana.jl:311)
         assert oracle.mana_mixed(np.outer(psi, psi.conj())) == pytest.approx(np.log2(3) * oracle.mana_pure(psi),
                                                                              rel=1e-12)
 
