@@ -32,7 +32,7 @@ EXPORTS = [
     "hm_abi_version", "hm_create", "hm_destroy", "hm_last_error", "hm_set_stream", "hm_last_kernel_ms",
     "hm_sre", "hm_sre_dev", "hm_sre_range", "hm_sre_range_dev", "hm_sre_batched", "hm_sre_grad",
     "hm_mc_sre", "hm_mana_pure", "hm_mana_mixed", "hm_gray_table", "hm_gray_table_general", "hm_set_param",
-    "hm_last_launch_count", "hm_probe_fp64_peak",
+    "hm_last_launch_count", "hm_probe_fp64_peak", "hm_sre_noalloc",
 ]
 HM_PARAM_BATCH = 1
 HM_PARAM_RING = 2
@@ -91,6 +91,7 @@ def load_library(path=None):
         L.hm_set_param.argtypes = [i, i]
         L.hm_last_launch_count.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong)]
         L.hm_probe_fp64_peak.argtypes = [_vp, _dp]
+        L.hm_sre_noalloc.argtypes = [_dp, i, _dp, i, _dp, _dp, _vp]
         for name in EXPORTS:
             if name != "hm_last_error" and name != "hm_abi_version":
                 getattr(L, name).restype = i

@@ -135,6 +135,27 @@ int hm_sre_batched(hm_ctx *ctx, int nstates, const double *const *psis, const in
  * stored.  psi host pointer, 1 <= n <= 21, q integer in [1, 8]. */
 int hm_sre_grad(hm_ctx *ctx, const double *psi, int n, double q, double *out_sre, double *grad);
 
+/* Exact SRE for callers that cannot allocate device memory.  No counterpart in the
+ * reference.  Some hosts cannot call cudaMalloc at all: code running inside another
+ * framework's memory pool, plugins that must not grow the device footprint after start-
+ * up, processes whose device memory is fully reserved by an allocator they do not own.
+ * This entry point allocates nothing: no context, no cudaMalloc / cudaFree, no pinned
+ * host buffers.  Its scratch (the device copy of the state, per-warp partial sums, the
+ * folded result; about 400 KB) is a fixed array inside the library, which every GPU that
+ * loads the library keeps until the process exits.
+ *   psi: host pointer, 2^n interleaved complex doubles, 1 <= n <= HM_NOALLOC_MAX_N (11);
+ *   larger n returns HM_ERR_SIZE and computes nothing.  qs[0..nq), 1 <= nq <= 4, q in
+ *   [1, 16].  Results as hm_sre (FP64): out_sre[i], out_lost[0], in host memory.
+ *   cuda_stream: the stream to run on (NULL = the legacy default stream); the call
+ *   returns after synchronising it.  Runs on the calling thread's current device.
+ * The first call on a device looks up the scratch array's device address; make that
+ * first call before any stream capture.  Every call on a device shares the one array and
+ * it keeps the last call's contents, so calls that overlap on the GPU (other threads,
+ * other streams) race: serialise them. */
+#define HM_NOALLOC_MAX_N 11
+int hm_sre_noalloc(const double *psi, int n, const double *qs, int nq, double *out_sre, double *out_lost,
+                   void *cuda_stream);
+
 /* ---------------------------------------------------------------------------------- */
 /* MC_SRE                                                                               */
 /* ---------------------------------------------------------------------------------- */
