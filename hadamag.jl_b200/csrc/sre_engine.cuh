@@ -138,6 +138,8 @@ __device__ __noinline__ void lane_moments_gen(const V *sm, int lane, double *s, 
 
 // Both precisions take the powers and the sums in FP64: an FP32 value of F converts to
 // double exactly, so the FP32 path's only roundings are those of f and of the butterflies.
+// NA interleaved accumulators per sum (value j goes to accumulator j mod NA, combined
+// pairwise at the end) keep the dependent-add chains short; the order is fixed.
 template <int R, int QS, typename V>
 __device__ __forceinline__ void lane_moments(const V (&v)[R], double *s, const QParams &qp, V *sm, int lane) {
   if constexpr (QS == QS_GEN) {
@@ -147,21 +149,33 @@ __device__ __forceinline__ void lane_moments(const V (&v)[R], double *s, const Q
     __syncwarp();
     return;
   } else {
-    double a2 = 0.0, a4 = 0.0, a6 = 0.0;
+    constexpr int NA = 4;
+    double a2[NA], a4[NA], a6[NA];
+#pragma unroll
+    for (int t = 0; t < NA; ++t) a2[t] = a4[t] = a6[t] = 0.0;
 #pragma unroll
     for (int i = 0; i < R; ++i) {
 #pragma unroll
       for (int c = 0; c < 2; ++c) {
         const double f = c ? (double)v[i].y : (double)v[i].x;
         const double y = f * f;
-        a2 += y;
-        a4 = fma(y, y, a4);
-        if constexpr (QS == QS_Q23) a6 = fma(y * y, y, a6);
+        const int t = (2 * i + c) % NA;
+        a2[t] += y;
+        a4[t] = fma(y, y, a4[t]);
+        if constexpr (QS == QS_Q23) a6[t] = fma(y * y, y, a6[t]);
       }
     }
-    s[0] = a2;
-    s[1] = a4;
-    if constexpr (QS == QS_Q23) s[2] = a6;
+#pragma unroll
+    for (int w = NA / 2; w > 0; w >>= 1)
+#pragma unroll
+      for (int t = 0; t < w; ++t) {
+        a2[t] += a2[t + w];
+        a4[t] += a4[t + w];
+        a6[t] += a6[t + w];
+      }
+    s[0] = a2[0];
+    s[1] = a4[0];
+    if constexpr (QS == QS_Q23) s[2] = a6[0];
   }
 }
 
@@ -275,6 +289,64 @@ __device__ __forceinline__ void p1_unit(const V *__restrict__ psi, const XInfo &
     const uint32_t p = (uint32_t)(i * 32 + lane);
     const uint32_t t = p >> LOGC, c = p & ((1u << LOGC) - 1u);
     __stcg(inter_x + (((size_t)t << (HI + LOGC)) + (rho << LOGC) + c), v[i]);
+  }
+}
+
+// ---------------------------------------------------------------------------------
+// Pass-1 output through the tensor-memory-access unit.  The row's 2^PB positions land in
+// 2^PB / C different pass-2 tiles, C positions each (C = 2 at n = 20): a warp-wide
+// st.global of them touches 16 cache lines per instruction.  Instead the warp writes the
+// row to its shared buffer in position order (conflict-free) and one thread issues
+// tensor stores that scatter it to the tile-major ring (no multicast; the ring is this
+// GPU's memory).  The 4-D tensor view of the ring, in scalars: d0 = the 2C scalars of a
+// tile row, d1 = the 2^HI rows, d2 = the 2^PB / C tiles, d3 = the 2X (slot, X-string)
+// pairs; boxes are {b0, 1, b2, 1}.
+struct TmaGeom {
+  int box0;  // scalars per box along d0 (2C, or 256 when 2C > 256)
+  int nb0;   // boxes along d0 per tile (2C / box0)
+  int box2;  // tiles per box (1 when nb0 > 1)
+  int nb2;   // box groups along the tiles
+  int C;     // positions per tile row
+};
+
+__device__ __forceinline__ void fence_proxy_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void tma_store_4d(const void *tmap, const void *smem_src, int c0, int c1, int c2, int c3) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_src);
+  asm volatile("cp.async.bulk.tensor.4d.global.shared::cta.bulk_group [%0, {%2, %3, %4, %5}], [%1];" ::"l"(tmap),
+               "r"(s), "r"(c0), "r"(c1), "r"(c2), "r"(c3)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// the shared-memory source of every committed store has been read
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// every committed store has completed
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+
+// As p1_unit, with the row leaving through the warp's shared buffer and tensor stores.
+// The caller waits for the stores to have read the buffer (bulk_wait_read_all on lane 0,
+// then __syncwarp) before the buffer's next use.
+template <int R, int HI, typename V>
+__device__ __forceinline__ void p1_unit_tma(const V *__restrict__ psi, const XInfo &xi, uint64_t rho, V *sm, int lane,
+                                            const void *tmap, const TmaGeom &g, int xcoord) {
+  constexpr int LOGR = ilog2c(R);
+  V v[R];
+  p1_build<R, false>(v, psi, xi, rho, sm, lane);
+  reg_wht<R, 0, LOGR>(v);
+  transpose_ab<R>(v, sm, lane);
+  reg_wht<R, 0, 5>(v);
+  // register i of lane l holds element k = R l + i, kept at position p = 32 i + l
+#pragma unroll
+  for (int i = 0; i < R; ++i) sm[i * 32 + lane] = v[i];
+  fence_proxy_async_smem();
+  __syncwarp();
+  if (lane == 0) {
+    for (int b2 = 0; b2 < g.nb2; ++b2)
+      for (int b0 = 0; b0 < g.nb0; ++b0)
+        tma_store_4d(tmap, sm + (size_t)b2 * g.box2 * g.C + (size_t)b0 * (g.box0 / 2), b0 * g.box0, (int)rho,
+                     b2 * g.box2, xcoord);
+    bulk_commit();
   }
 }
 

@@ -1,6 +1,9 @@
 // sre_host.cu -- exact-SRE driver: precision dispatch, fold of the per-warp partials,
 // result read-back.
+#include <cudaTypedefs.h>
 #include <math.h>
+
+#include <mutex>
 
 #include "sre_launch.cuh"
 
@@ -25,6 +28,43 @@ static int launch_sre_prec(hm_ctx *c, const void *psi_dev, int n, uint64_t kb, u
 TwoPassCfg &twopass_cfg() {
   static TwoPassCfg cfg;
   return cfg;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link-time
+// dependency on libcuda), looked up once per process.
+static PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+bool encode_ring_tmap(CUtensorMap *m, void *ring, int scalar_bytes, int C, int U, int T, int two_x,
+                      uint64_t x_stride_bytes, const TmaGeom &g) {
+  // innermost box extent and every stride must be multiples of 16 bytes; boxes <= 256
+  const uint64_t row_bytes = (uint64_t)2 * C * scalar_bytes;
+  if ((g.box0 * scalar_bytes) % 16 != 0 || row_bytes % 16 != 0 || g.box0 > 256 || g.box2 > 256) return false;
+  if (g.nb0 * g.box0 != 2 * C || g.nb2 * g.box2 != T) return false;
+  if (((uintptr_t)ring & 15) != 0) return false;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+  if (!enc) return false;
+  const cuuint64_t dims[4] = {(cuuint64_t)2 * C, (cuuint64_t)U, (cuuint64_t)T, (cuuint64_t)two_x};
+  const cuuint64_t strides[3] = {row_bytes, row_bytes * (uint64_t)U, x_stride_bytes};
+  const cuuint32_t box[4] = {(cuuint32_t)g.box0, 1u, (cuuint32_t)g.box2, 1u};
+  const cuuint32_t estr[4] = {1u, 1u, 1u, 1u};
+  const CUresult r =
+      enc(m, scalar_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, ring, dims,
+          strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS;
 }
 
 __global__ void k_fold_partials(const double *__restrict__ partials, int nwarps, int nsum, double *out) {

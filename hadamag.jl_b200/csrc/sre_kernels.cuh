@@ -1,6 +1,8 @@
 // sre_kernels.cuh -- exact-SRE kernels (fused single-warp sweep for n <= PB+1, and the
 // two-pass stage kernels for larger n) plus the deterministic double-double fold.
 #pragma once
+#include <cuda.h>  // CUtensorMap
+
 #include "sre_engine.cuh"
 
 namespace hm {
@@ -106,6 +108,7 @@ __global__ void __launch_bounds__(FUSED_WARPS * 32) k_sre_fused(SreArgs a) {
 template <typename T> struct StageOcc { static constexpr int value = sizeof(T) == 8 ? 2 : 4; };
 
 struct StageArgs {
+  CUtensorMap tmap;    // tensor view of the ring for the pass-1 stores (valid when tma)
   const void *psi;
   const void *psi_sw[16];
   void *ring;          // 2 slots x X strings x 2^(n-1) V
@@ -113,14 +116,17 @@ struct StageArgs {
   unsigned *stage;     // [0] stage index, [1] CTAs finished in the current stage
   uint64_t k_begin, k_end;
   QParams qp;
-  int n, X, nbatch;
+  TmaGeom g;
+  int n, X, nbatch, tma;
 };
 
 template <typename T, int R, int HI, int QS>
-__global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value) k_sre_stage(StageArgs a) {
+__global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
+    k_sre_stage(const __grid_constant__ StageArgs a) {
   using V = typename VT<T>::V;
   constexpr int LOGR = ilog2c(R), PB = LOGR + 5, NQ = QSet<QS>::NQ;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
+  // the tensor stores read the per-warp buffers: keep them 1024-byte aligned
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   V *sm = reinterpret_cast<V *>(smem_raw) + warp * (32 * R);
   const long long t = (long long)*(volatile unsigned *)a.stage;
@@ -148,9 +154,17 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value) k_sre_stag
     V *inter_x = ring + ((size_t)(b & 1) * a.X + xs) * xlen;
     const XInfo xi = make_xinfo(k, a.k_end, n, PB);
     if (!xi.active) continue;
+    if (a.tma) {
+      // the previous unit's tensor stores must have read the shared buffer
+      if (lane == 0) bulk_wait_read_all();
+      __syncwarp();
+    }
     if (!p2) {
       const V *src = xi.sw < 0 ? psi : reinterpret_cast<const V *>(a.psi_sw[xi.sw]);
-      p1_unit<R, HI, false>(src, xi, sub, inter_x, sm, lane);
+      if (a.tma)
+        p1_unit_tma<R, HI>(src, xi, sub, sm, lane, &a.tmap, a.g, (int)((b & 1) * a.X + xs));
+      else
+        p1_unit<R, HI, false>(src, xi, sub, inter_x, sm, lane);
     } else {
       double s[NQ + 1];
       p2_unit<R, HI, QS>(inter_x + (sub << PB), sm, lane, s, a.qp);
@@ -171,6 +185,8 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value) k_sre_stag
       sl[2 * q + 1] = v.lo;
     }
   }
+  // the ring rows this warp stored are complete before the stage is reported done
+  if (a.tma && lane == 0) bulk_wait_all();
   // the last CTA of the stage advances the stage index for the next launch
   __syncthreads();
   if (threadIdx.x == 0) {

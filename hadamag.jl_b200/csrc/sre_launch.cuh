@@ -20,6 +20,24 @@ struct TwoPassCfg {
 
 TwoPassCfg &twopass_cfg();
 
+// Tensor map of the two-pass ring for the pass-1 tensor stores (see p1_unit_tma):
+// scalar_bytes 8 (FP64) or 4 (FP32), C positions per tile row, U = 2^HI rows, T tiles,
+// two_x = 2X (slot, X-string) pairs, x_stride_bytes = 2^(n-1) complex.  Returns false
+// (and leaves the plain stores in use) when the geometry does not meet the unit's rules
+// or the driver does not provide the encoder.
+bool encode_ring_tmap(CUtensorMap *m, void *ring, int scalar_bytes, int C, int U, int T, int two_x,
+                      uint64_t x_stride_bytes, const TmaGeom &g);
+
+inline TmaGeom ring_tma_geom(int C, int T) {
+  TmaGeom g;
+  g.C = C;
+  g.box0 = 2 * C <= 256 ? 2 * C : 256;
+  g.nb0 = 2 * C / g.box0;
+  g.box2 = g.nb0 > 1 ? 1 : (T < 256 ? T : 256);
+  g.nb2 = T / g.box2;
+  return g;
+}
+
 template <typename T, int R, int NB, int QS>
 static int launch_fused(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
   using V = typename VT<T>::V;
@@ -75,6 +93,11 @@ static int launch_stages(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
   const size_t ring_bytes = 2 * (size_t)X * per_x;
   HM_TRY(ensure_dev(c, &c->d_inter, &c->inter_cap, ring_bytes));
   a.ring = c->d_inter;
+  {
+    constexpr int C = 1 << (PB - HI), NT = (1 << PB) / C;
+    a.g = ring_tma_geom(C, NT);
+    a.tma = encode_ring_tmap(&a.tmap, a.ring, (int)sizeof(T), C, 1 << HI, NT, 2 * (int)X, per_x, a.g) ? 1 : 0;
+  }
   if (a.k_begin < (1ull << PB)) {
     const size_t slen = (size_t)1 << a.n;
     HM_TRY(ensure_dev(c, &c->d_aux2, &c->aux2_cap, (size_t)PB * slen * sizeof(V)));

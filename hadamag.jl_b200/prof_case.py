@@ -1,0 +1,41 @@
+"""Small exact-SRE workload for kernel profiling (ncu) and quick timing.
+
+Runs hm_sre_range on a slice of Gray indices of a seeded N-qubit state, so that one
+profiled launch of the two-pass stage kernel sees the full-size transform (2^(N-1)
+points per X-string) while the whole run stays short:
+
+    python hadamag.jl_b200/prof_case.py --n 20 --k0 1024 --count 256 --precision fp64
+
+Prints the sums and the device time of the call.
+"""
+import argparse
+import os
+import sys
+
+import numpy as np
+
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+import hadamag_b200 as hm  # noqa: E402
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--n", type=int, default=20)
+    ap.add_argument("--k0", type=int, default=1024, help="first Gray index")
+    ap.add_argument("--count", type=int, default=256, help="number of X-strings")
+    ap.add_argument("--precision", default="fp64", choices=sorted(hm.PRECISIONS))
+    ap.add_argument("--q", type=float, nargs="+", default=[2.0])
+    ap.add_argument("--repeat", type=int, default=2)
+    args = ap.parse_args()
+    g = np.random.default_rng(args.n)
+    psi = g.normal(size=1 << args.n) + 1j * g.normal(size=1 << args.n)
+    psi /= np.linalg.norm(psi)
+    ctx = hm._native.default_context(0)
+    for _ in range(args.repeat):
+        p2, m = ctx.sre_range(psi, args.k0, args.k0 + args.count, tuple(args.q), hm.PRECISIONS[args.precision])
+    print(f"n={args.n} k=[{args.k0},{args.k0 + args.count}) p2={p2.sum():.17g} m={m.sum(axis=1)} "
+          f"kernel_ms={ctx.last_kernel_ms():.3f} launches={ctx.last_launch_count()}")
+
+
+if __name__ == "__main__":
+    main()

@@ -43,7 +43,7 @@ extern "C" {
 
 /* precision / algorithm selector for the exact-SRE entry points */
 #define HM_FP64 0  /* FP64 butterflies, FP64 double-double reduction            */
-#define HM_FP32 1  /* FP32 butterflies, FP32 per-lane partials, FP64 reduction  */
+#define HM_FP32 1  /* FP32 butterflies, FP64 powers and reduction               */
 #define HM_PLAIN 2 /* the reference CUDA backend's launch structure, FP64       */
 
 typedef struct hm_ctx hm_ctx;
