@@ -249,6 +249,13 @@ def Mana(psi, backend="auto", progress=False, device=0):
     return be.context().mana_pure(s.data)
 
 
+def autotune(n, precision="fp64", device=0):
+    """Time the exact-SRE sweep of an n-qubit state for several batch sizes and keep the
+    fastest for later calls of that size and precision (12 <= n <= 21).  Returns
+    (batch size, microseconds per X-string).  No reference counterpart."""
+    return default_context(device).autotune(n, _precision(precision))
+
+
 def generate_gray_table(n, q):
     """Gray table as src/Basis.jl:252-265, computed on the device.
 

@@ -32,7 +32,7 @@ EXPORTS = [
     "hm_abi_version", "hm_create", "hm_destroy", "hm_last_error", "hm_set_stream", "hm_last_kernel_ms",
     "hm_sre", "hm_sre_dev", "hm_sre_range", "hm_sre_range_dev", "hm_sre_batched", "hm_sre_grad",
     "hm_mc_sre", "hm_mana_pure", "hm_mana_mixed", "hm_gray_table", "hm_gray_table_general", "hm_set_param",
-    "hm_last_launch_count", "hm_probe_fp64_peak", "hm_sre_noalloc",
+    "hm_last_launch_count", "hm_probe_fp64_peak", "hm_sre_noalloc", "hm_autotune",
 ]
 HM_PARAM_BATCH = 1
 HM_PARAM_RING = 2
@@ -92,6 +92,7 @@ def load_library(path=None):
         L.hm_last_launch_count.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong)]
         L.hm_probe_fp64_peak.argtypes = [_vp, _dp]
         L.hm_sre_noalloc.argtypes = [_dp, i, _dp, i, _dp, _dp, _vp]
+        L.hm_autotune.argtypes = [_vp, i, i, _ip, _dp]
         for name in EXPORTS:
             if name != "hm_last_error" and name != "hm_abi_version":
                 getattr(L, name).restype = i
@@ -151,6 +152,15 @@ class Context:
         v = ctypes.c_double()
         self._check(self.lib.hm_probe_fp64_peak(self.handle, ctypes.byref(v)), "hm_probe_fp64_peak")
         return v.value
+
+    def autotune(self, n, precision=HM_FP64):
+        """Pick and record the two-pass batch size for (n, precision); returns
+        (X, microseconds per X-string)."""
+        x = ctypes.c_int()
+        us = ctypes.c_double()
+        self._check(self.lib.hm_autotune(self.handle, int(n), int(precision), ctypes.byref(x), ctypes.byref(us)),
+                    "hm_autotune")
+        return x.value, us.value
 
     def last_kernel_ms(self):
         v = ctypes.c_double()

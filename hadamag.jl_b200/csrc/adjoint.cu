@@ -325,8 +325,9 @@ int run_sre_grad(hm_ctx *c, const double2 *psi, int n, int q, double *m_out, dou
   a.cq_x = 2.0 * q * pow(4.0, q);
   a.cq_0 = 2.0 * q;
   const uint64_t len = 1ull << n;
-  // chunk: G of at most 64 MiB
-  int chunk = (int)std::max<uint64_t>(1, ((uint64_t)64 << 20) / (len * sizeof(double2)));
+  // chunk: G of at most 1 GiB.  Each chunk costs four launches; with small chunks (16
+  // X-strings at n = 18 for 64 MiB) the launches were under-filled and dominated the time
+  int chunk = (int)std::max<uint64_t>(1, ((uint64_t)1 << 30) / (len * sizeof(double2)));
   if ((uint64_t)chunk > len) chunk = (int)len;
   a.chunk = chunk;
   HM_TRY(ensure_dev(c, &c->d_inter, &c->inter_cap, (size_t)chunk * len * sizeof(double2) +

@@ -205,6 +205,73 @@ int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, 
 
 }  // namespace hm
 
+// Fill psi with a unit-norm pattern state (values do not matter for timing).
+static __global__ void k_tune_state(double2 *psi, uint64_t len) {
+  const double s = rsqrt((double)len);
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < len; i += (uint64_t)gridDim.x * blockDim.x) {
+    double sn, cs;
+    sincospi((double)(i % 977) / 977.0 * 2.0, &sn, &cs);
+    psi[i] = make_double2(s * cs, s * sn);
+  }
+}
+
+// Autotuner of the two-pass batch size: time hm_sre_range on `sample` Gray indices
+// (starting at 1024, where the sweep's steady state begins) for X = 1, 2, 4, ... while
+// the ring stays within 1 GiB, keep the fastest, and record it for this (n, precision).
+extern "C" int hm_autotune(hm_ctx *c, int n, int precision, int *best_x, double *best_us_per_x) {
+  if (!c) return HM_ERR_ARG;
+  c->err.clear();
+  if (!best_x || !best_us_per_x) return hm::set_err(c, HM_ERR_ARG, "null output pointer");
+  if (n < 12 || n > 21) return hm::set_err(c, HM_ERR_SIZE, "autotune: n = %d outside the two-pass range [12, 21]", n);
+  if (precision != HM_FP64 && precision != HM_FP32)
+    return hm::set_err(c, HM_ERR_ARG, "autotune: precision must be HM_FP64 or HM_FP32");
+  HM_CUDA(c, cudaSetDevice(c->device));
+  const uint64_t len = 1ull << n;
+  HM_TRY(hm::ensure_dev(c, &c->d_psi, &c->psi_cap, len * sizeof(double2)));
+  k_tune_state<<<c->num_sms * 4, 256, 0, c->stream>>>((double2 *)c->d_psi, len);
+  HM_CUDA(c, cudaGetLastError());
+  hm::TwoPassCfg &cfg = hm::twopass_cfg();
+  const hm::TwoPassCfg saved = cfg;
+  const int pi = precision == HM_FP64 ? 0 : 1;
+  const uint64_t per_x = (len / 2) * (precision == HM_FP64 ? sizeof(double2) : sizeof(float2));
+  const uint64_t rows = len / 2 / 1024;  // pass-1 units per X-string
+  // sample: at least 8 batches of the largest candidate and about 4096 pass-1 units
+  uint64_t xmax = 1;
+  while (xmax < 256 && 2 * (xmax * 2) * per_x <= (1ull << 30)) xmax *= 2;
+  uint64_t sample = std::max<uint64_t>(8 * xmax, (8192 + rows - 1) / rows);
+  if (1024 + sample > len) sample = len - 1024;
+  hm::QReq q;
+  q.nq = 1;
+  q.q[0] = 2.0;
+  double dd[10], best = 1e300;
+  int bx = 0;
+  int rc = HM_OK;
+  for (uint64_t X = 1; X <= xmax && rc == HM_OK; X *= 2) {
+    cfg.X = (int)X;
+    cfg.X_set = 1;
+    cfg.ring_mib = std::max<int>(saved.ring_mib, (int)((2 * X * per_x + (1 << 20) - 1) >> 20));
+    double t = 1e300;
+    for (int rep = 0; rep < 2 && rc == HM_OK; ++rep) {
+      rc = hm::run_sre(c, (const double2 *)c->d_psi, n, 1024, 1024 + sample, q, precision, dd);
+      if (rc == HM_OK && rep > 0) t = std::min(t, c->last_ms);
+    }
+    if (rc == HM_OK && t < best) {
+      best = t;
+      bx = (int)X;
+    }
+  }
+  // restore the knobs; keep the result in the table
+  int tuned[2][32];
+  memcpy(tuned, cfg.tuned_x, sizeof tuned);
+  cfg = saved;
+  memcpy(cfg.tuned_x, tuned, sizeof tuned);
+  if (rc != HM_OK) return rc;
+  cfg.tuned_x[pi][n] = bx;
+  *best_x = bx;
+  *best_us_per_x = best * 1e3 / (double)sample;
+  return HM_OK;
+}
+
 extern "C" int hm_set_param(int param, int value) {
   hm::TwoPassCfg &cfg = hm::twopass_cfg();
   const hm::TwoPassCfg def;

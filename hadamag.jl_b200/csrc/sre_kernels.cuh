@@ -126,9 +126,9 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
   using V = typename VT<T>::V;
   constexpr int LOGR = ilog2c(R), PB = LOGR + 5, NQ = QSet<QS>::NQ;
   // the tensor stores read the per-warp buffers: keep them 1024-byte aligned
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  extern __shared__ __align__(1024) unsigned char smem_stage[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  V *sm = reinterpret_cast<V *>(smem_raw) + warp * (32 * R);
+  V *sm = reinterpret_cast<V *>(smem_stage) + warp * (32 * R);
   const long long t = (long long)*(volatile unsigned *)a.stage;
   if (t > a.nbatch) return;  // padding stages of the last graph replay
   const int gwarp = blockIdx.x * SRE_WARPS + warp;

@@ -6,16 +6,26 @@
 
 namespace hm {
 
-// Tunables of the two-pass stage kernels (the autotuner sets them through hm_set_param):
-// a batch holds about `units_target` warp units per pass (X = units_target / 2^HI
-// X-strings, or X when set explicitly), the two-batch ring stays within `ring_mib`
-// (L2 resident), and `graph_stages` stages are captured per CUDA graph.
+// Tunables of the two-pass stage kernels (set through hm_set_param): a batch holds about
+// `units_target` warp units per pass (X = units_target / 2^HI X-strings, or X when set
+// explicitly), the two-batch ring stays within `ring_mib`, and `graph_stages` stages are
+// captured per CUDA graph.  Every stage costs a fixed few microseconds (launch, the first
+// loads of all warps at once, the tail), so for the large FP64 sizes (2^HI >= 128 rows)
+// the default batch is `fp64_large_x` X-strings with a ring of up to `fp64_ring_mib`,
+// even though such a ring no longer fits in L2 (measured on B200 at n = 18 and 20:
+// X = 16 beats the L2-resident X = 4 by 10-40%).  Setting HM_PARAM_BATCH, _UNITS or
+// _RING switches to the generic rule.
 struct TwoPassCfg {
   int X = 0;
   int X_set = 0;
   int units_target = 4096;
   int ring_mib = 64;
   int graph_stages = 32;
+  int fp64_large_x = 16;
+  int fp64_ring_mib = 256;
+  // batch sizes chosen by hm_autotune, per precision (0 FP64, 1 FP32) and qubit count;
+  // 0 = not tuned.  Used when HM_PARAM_BATCH is not set.
+  int tuned_x[2][32] = {};
 };
 
 TwoPassCfg &twopass_cfg();
@@ -83,10 +93,24 @@ static int launch_stages(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
   a.n = a0.n;
   const uint64_t U = 1ull << HI;
   const uint64_t len = a.k_end - a.k_begin;
-  uint64_t X = cfg.X_set ? (uint64_t)cfg.X : std::max<uint64_t>(1, (uint64_t)cfg.units_target / U);
+  const TwoPassCfg def;
+  const bool generic = cfg.X_set || cfg.units_target != def.units_target || cfg.ring_mib != def.ring_mib;
+  uint64_t X, ring_mib = (uint64_t)cfg.ring_mib;
+  const int tuned = cfg.tuned_x[sizeof(T) == 8 ? 0 : 1][a.n];
+  if (cfg.X_set) {
+    X = (uint64_t)cfg.X;
+  } else if (tuned > 0) {
+    X = (uint64_t)tuned;
+    ring_mib = std::max<uint64_t>(ring_mib, (2 * X * ((uint64_t)1 << (a.n - 1)) * sizeof(V) + (1 << 20) - 1) >> 20);
+  } else if (!generic && sizeof(T) == 8 && U >= 128) {
+    X = (uint64_t)cfg.fp64_large_x;
+    ring_mib = (uint64_t)cfg.fp64_ring_mib;
+  } else {
+    X = std::max<uint64_t>(1, (uint64_t)cfg.units_target / U);
+  }
   // ring bytes 2 X 2^(n-1) sizeof(V) within the budget
   const uint64_t per_x = ((uint64_t)1 << (a.n - 1)) * sizeof(V);
-  while (X > 1 && 2 * X * per_x > ((uint64_t)cfg.ring_mib << 20)) X >>= 1;
+  while (X > 1 && 2 * X * per_x > (ring_mib << 20)) X >>= 1;
   if (X > len) X = len;
   a.X = (int)X;
   a.nbatch = (int)((len + X - 1) / X);

@@ -78,6 +78,13 @@ int hm_set_stream(hm_ctx *ctx, void *cuda_stream);
 #define HM_PARAM_GRAPH 4
 int hm_set_param(int param, int value);
 
+/* Autotuner of the two-pass sweep (no reference counterpart): times the sweep of an n-qubit
+ * state for batch sizes X = 1, 2, 4, ... (ring up to 1 GiB) on a sample of Gray indices,
+ * records the fastest X for this (n, precision) in a process-wide table that later calls
+ * use unless HM_PARAM_BATCH is set, and returns it with the measured microseconds per
+ * X-string.  12 <= n <= 21, precision HM_FP64 or HM_FP32.  Takes a fraction of a second. */
+int hm_autotune(hm_ctx *ctx, int n, int precision, int *best_x, double *best_us_per_x);
+
 /* Number of kernels the last call launched on the device (graph nodes included). */
 int hm_last_launch_count(hm_ctx *ctx, long long *count);
 

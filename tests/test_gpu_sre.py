@@ -130,3 +130,16 @@ def test_batched_matches_per_state(ctx, hm, oracle):
         for i, p in enumerate(psis):
             assert vals[i, 0] == close(oracle.sre(p, 2)[0], prec)
             assert vals[i, 1] == close(oracle.sre(p, 3)[0], prec)
+
+
+def test_autotune_records_a_batch_size(ctx, hm, oracle):
+    n = 13
+    psi = rand_state(1 << n, 77)
+    ref = oracle.sre(psi, 2)[0]
+    for prec in ("fp64", "fp32"):
+        x, us = ctx.autotune(n, hm.PRECISIONS[prec])
+        assert x >= 1 and (x & (x - 1)) == 0 and us > 0
+        v, _ = ctx.sre(psi, (2.0,), hm.PRECISIONS[prec])  # runs with the tuned batch size
+        assert v[0] == close(ref, prec)
+    with pytest.raises(hm.ArgumentError):
+        ctx.autotune(11, hm.HM_FP64)
