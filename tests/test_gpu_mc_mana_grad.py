@@ -67,11 +67,11 @@ def test_mana_mixed_reduced_10_qutrits(hm, oracle):
     assert abs(hm.Mana(hm.DensityMatrix(np.eye(729) / 729, q=3))) < 1e-12
 
 
-@pytest.mark.parametrize("n", [1, 3, 6, 9, 11, 12, 13])
-def test_grad_matches_oracle(ctx, oracle, n):
+@pytest.mark.parametrize("n,q", [(1, 2), (3, 2), (6, 2), (9, 2), (11, 2), (12, 2), (13, 2), (14, 2), (12, 3)])
+def test_grad_matches_oracle(ctx, oracle, n, q):
     psi = rand_state(1 << n, 500 + n)
-    v, g = ctx.sre_grad(psi, 2)
-    ov, og = oracle.sre_grad(psi, 2)
+    v, g = ctx.sre_grad(psi, q)
+    ov, og = oracle.sre_grad(psi, q)
     assert v == pytest.approx(ov, rel=1e-10)
     assert np.max(np.abs(g - og)) <= 1e-10 * np.max(np.abs(og))
 
