@@ -168,6 +168,15 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
     } else {
       double s[NQ + 1];
       p2_unit<R, HI, QS>(inter_x + (sub << PB), sm, lane, s, a.qp);
+      // The tile is dead once read (its slot is rewritten by pass 1 two stages later, in
+      // another launch): drop its L2 lines without writing them back to DRAM.
+      {
+        const char *tb = reinterpret_cast<const char *>(inter_x + (sub << PB));
+        constexpr int LINES = (int)(32 * R * sizeof(V) / 128);
+#pragma unroll
+        for (int ln = lane; ln < LINES; ln += 32)
+          asm volatile("discard.global.L2 [%0], 128;" ::"l"(tb + (size_t)ln * 128) : "memory");
+      }
       s[0] = 4.0 * s[0];
 #pragma unroll
       for (int q = 0; q < NQ; ++q) s[1 + q] *= q_scale<QS>(q, false, a.qp);

@@ -10,19 +10,25 @@ namespace hm {
 // `units_target` warp units per pass (X = units_target / 2^HI X-strings, or X when set
 // explicitly), the two-batch ring stays within `ring_mib`, and `graph_stages` stages are
 // captured per CUDA graph.  Every stage costs a fixed few microseconds (launch, the first
-// loads of all warps at once, the tail), so for the large FP64 sizes (2^HI >= 128 rows)
-// the default batch is `fp64_large_x` X-strings with a ring of up to `fp64_ring_mib`,
-// even though such a ring no longer fits in L2 (measured on B200 at n = 18 and 20:
-// X = 16 beats the L2-resident X = 4 by 10-40%).  Setting HM_PARAM_BATCH, _UNITS or
-// _RING switches to the generic rule.
+// loads of all warps at once, the tail), which favours large batches, while a ring that
+// outgrows the 126 MB L2 costs DRAM traffic.  Where they pull apart (n >= 18) the default
+// batch comes from `measured_x`, timed on B200 (us per X-string, discarded dead tiles):
+//   FP64  n = 18: X = 32 (0.98; X = 16 1.14)   n = 20: X = 16 (4.38; X = 4 4.75)
+//         n = 21: X = 2  (13.6; X = 8 22.4)
+//   FP32  n = 18: X = 64 (0.52)   n = 20: X = 8 (3.09; X = 16 3.47)   n = 21: X = 8 (10.8)
+// (n = 19 interpolated).  hm_autotune measures and records a batch for the machine at
+// hand; setting HM_PARAM_BATCH, _UNITS or _RING switches to the generic rule.
+inline int measured_x(bool fp64, int n) {
+  static const int f64[4] = {32, 16, 16, 2}, f32[4] = {64, 16, 8, 8};
+  return (n >= 18 && n <= 21) ? (fp64 ? f64 : f32)[n - 18] : 0;
+}
+
 struct TwoPassCfg {
   int X = 0;
   int X_set = 0;
   int units_target = 4096;
   int ring_mib = 64;
   int graph_stages = 32;
-  int fp64_large_x = 16;
-  int fp64_ring_mib = 256;
   // batch sizes chosen by hm_autotune, per precision (0 FP64, 1 FP32) and qubit count;
   // 0 = not tuned.  Used when HM_PARAM_BATCH is not set.
   int tuned_x[2][32] = {};
@@ -97,14 +103,12 @@ static int launch_stages(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
   const bool generic = cfg.X_set || cfg.units_target != def.units_target || cfg.ring_mib != def.ring_mib;
   uint64_t X, ring_mib = (uint64_t)cfg.ring_mib;
   const int tuned = cfg.tuned_x[sizeof(T) == 8 ? 0 : 1][a.n];
+  const int measured = generic ? 0 : measured_x(sizeof(T) == 8, a.n);
   if (cfg.X_set) {
     X = (uint64_t)cfg.X;
-  } else if (tuned > 0) {
-    X = (uint64_t)tuned;
+  } else if (tuned > 0 || measured > 0) {
+    X = (uint64_t)(tuned > 0 ? tuned : measured);
     ring_mib = std::max<uint64_t>(ring_mib, (2 * X * ((uint64_t)1 << (a.n - 1)) * sizeof(V) + (1 << 20) - 1) >> 20);
-  } else if (!generic && sizeof(T) == 8 && U >= 128) {
-    X = (uint64_t)cfg.fp64_large_x;
-    ring_mib = (uint64_t)cfg.fp64_ring_mib;
   } else {
     X = std::max<uint64_t>(1, (uint64_t)cfg.units_target / U);
   }

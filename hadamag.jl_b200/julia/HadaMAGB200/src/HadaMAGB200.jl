@@ -10,6 +10,7 @@ libhadamag_b200.so (C ABI declared in include/hadamag_b200.h).
     Mana(ψ3; backend = HadaMAGB200.B200())
     HadaMAGB200.Mana(ρ)                       # DensityMatrix{ComplexF64,3}
     HadaMAGB200.SRE_grad(ψ, 2)                # value and dSRE/dψ (no reference counterpart)
+    Zygote.gradient(v -> HadaMAGB200.sre_value(v, 2), data(ψ))   # through the rrule
 
 Passing the backend object works with the unmodified package: `_choose_backend` gets a
 method for `B200` and `_apply_backend` routes to the functions below (the dispatch of
@@ -26,6 +27,7 @@ module HadaMAGB200
 
 using HadaMAG
 using Random
+using ChainRulesCore
 
 const LIB = Ref{String}(joinpath(@__DIR__, "..", "..", "..", "libhadamag_b200.so"))
 const CTX = Ref{Ptr{Cvoid}}(C_NULL)
@@ -131,6 +133,38 @@ function SRE_grad(ψ, q = 2)
                context(), reinterpret(Float64, v), qubits(ψ), Float64(q), val, reinterpret(Float64, g))
     check(rc, "hm_sre_grad")
     return (val[], g)
+end
+
+"""
+    sre_value(v::AbstractVector{ComplexF64}, q = 2) -> Float64
+
+SRE_q of the normalised amplitude vector `v` (length 2^n) as a plain differentiable
+function: its `ChainRulesCore.rrule` runs the adjoint kernel (`hm_sre_grad`) once and
+returns the value with a pullback.  For a real function of complex input the cotangent
+is dSRE/dRe v + im dSRE/dIm v, which is what the kernel produces.
+"""
+function sre_value(v::AbstractVector{ComplexF64}, q = 2)
+    out = zeros(Float64, 1)
+    lost = Ref{Float64}(0.0)
+    w = collect(v)
+    rc = ccall((:hm_sre, LIB[]), Cint,
+               (Ptr{Cvoid}, Ptr{Float64}, Cint, Ptr{Float64}, Cint, Cint, Ptr{Float64}, Ref{Float64}),
+               context(), reinterpret(Float64, w), trailing_zeros(length(w)), Float64[q], 1, HM_FP64, out, lost)
+    check(rc, "hm_sre")
+    return out[1]
+end
+
+function ChainRulesCore.rrule(::typeof(sre_value), v::AbstractVector{ComplexF64}, q)
+    w = collect(v)
+    g = similar(w)
+    val = Ref{Float64}(0.0)
+    rc = ccall((:hm_sre_grad, LIB[]), Cint,
+               (Ptr{Cvoid}, Ptr{Float64}, Cint, Cdouble, Ref{Float64}, Ptr{Float64}),
+               context(), reinterpret(Float64, w), trailing_zeros(length(w)), Float64(q), val,
+               reinterpret(Float64, g))
+    check(rc, "hm_sre_grad")
+    sre_pullback(ȳ) = (NoTangent(), ȳ .* g, NoTangent())
+    return val[], sre_pullback
 end
 
 HadaMAG._choose_backend(b::B200) = b
