@@ -273,15 +273,22 @@ __device__ __forceinline__ void p1_build(V (&v)[R], const V *__restrict__ psi, c
 //   inter_x[t * 2^(HI+LOGC) + row * C + c]  for pass-2 tile t, row, column c < C,
 // so that a pass-2 tile is one contiguous 2^PB-element block and pass 1 writes whole
 // 32-byte sectors (C >= 2).
-template <int R, int HI, bool STAGE_B, typename V>
+// Hook run by every lane right before a pass-1 unit's first global store (the stage
+// kernels wait there for the previous stage); the default does nothing.
+struct NoHook {
+  __device__ __forceinline__ void operator()() const {}
+};
+
+template <int R, int HI, bool STAGE_B, typename V, typename Pre = NoHook>
 __device__ __forceinline__ void p1_unit(const V *__restrict__ psi, const XInfo &xi, uint64_t rho,
-                                        V *__restrict__ inter_x, V *sm, int lane) {
+                                        V *__restrict__ inter_x, V *sm, int lane, const Pre &pre = Pre()) {
   constexpr int LOGR = ilog2c(R), PB = LOGR + 5, LOGC = PB - HI;
   V v[R];
   p1_build<R, STAGE_B>(v, psi, xi, rho, sm, lane);
   reg_wht<R, 0, LOGR>(v);  // element bits 5 .. PB-1
   transpose_ab<R>(v, sm, lane);
   reg_wht<R, 0, 5>(v);  // element bits 0 .. 4
+  pre();
   // register i of lane l holds element k = R l + i; it is stored at position p = 32 i + l
   // of the row (any fixed relabelling of k is invisible to the moment sums)
 #pragma unroll
@@ -327,9 +334,9 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 // As p1_unit, with the row leaving through the warp's shared buffer and tensor stores.
 // The caller waits for the stores to have read the buffer (bulk_wait_read_all on lane 0,
 // then __syncwarp) before the buffer's next use.
-template <int R, int HI, typename V>
+template <int R, int HI, typename V, typename Pre = NoHook>
 __device__ __forceinline__ void p1_unit_tma(const V *__restrict__ psi, const XInfo &xi, uint64_t rho, V *sm, int lane,
-                                            const void *tmap, const TmaGeom &g, int xcoord) {
+                                            const void *tmap, const TmaGeom &g, int xcoord, const Pre &pre = Pre()) {
   constexpr int LOGR = ilog2c(R);
   V v[R];
   p1_build<R, false>(v, psi, xi, rho, sm, lane);
@@ -341,6 +348,7 @@ __device__ __forceinline__ void p1_unit_tma(const V *__restrict__ psi, const XIn
   for (int i = 0; i < R; ++i) sm[i * 32 + lane] = v[i];
   fence_proxy_async_smem();
   __syncwarp();
+  pre();
   if (lane == 0) {
     for (int b2 = 0; b2 < g.nb2; ++b2)
       for (int b0 = 0; b0 < g.nb0; ++b0)

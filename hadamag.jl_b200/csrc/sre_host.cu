@@ -67,6 +67,8 @@ bool encode_ring_tmap(CUtensorMap *m, void *ring, int scalar_bytes, int C, int U
   return r == CUDA_SUCCESS;
 }
 
+__global__ void k_stage_advance(unsigned *stage, unsigned count) { stage[0] += count; }
+
 __global__ void k_fold_partials(const double *__restrict__ partials, int nwarps, int nsum, double *out) {
   // one block; thread t folds warps t, t + blockDim, ... then a fixed-shape tree
   __shared__ dd sh[256][5];

@@ -100,9 +100,14 @@ __global__ void __launch_bounds__(FUSED_WARPS * 32) k_sre_fused(SreArgs a) {
 // pass 2 of batch t - 1 (independent work: the kernel boundary is the only dependency),
 // with batch b's intermediate in ring slot b % 2.  Every warp walks a fixed round-robin
 // share of the stage's units and adds its moment sums into its own double-double slot,
-// so the result does not depend on scheduling.  The stage index lives in device memory:
-// the last CTA to finish a stage advances it, which lets a block of stages be captured
-// once as a CUDA graph and replayed.
+// so the result does not depend on scheduling.  A block of stages is captured once as a
+// CUDA graph and replayed: node `node` of the graph runs stage base + node, with `base`
+// in device memory, advanced by a one-thread kernel at the end of every replay.
+// The stage nodes are chained by programmatic dependent launch: stage t + 1 may start on
+// the SMs that stage t has already left.  It then runs the reads of psi and the
+// butterflies of its first pass-1 units, and waits for stage t to finish (and its memory
+// to be visible) only before its first access that depends on stage t: a ring store
+// (the slot that stage t's pass 2 reads), a ring load, the moment-slot update.
 // CTAs per SM of the stage kernels: FP64 keeps 32 complex (128 registers) of data per
 // lane and runs at 255 registers (8 warps / SM), FP32 at 128 registers (16 warps / SM)
 template <typename T> struct StageOcc { static constexpr int value = sizeof(T) == 8 ? 2 : 4; };
@@ -113,12 +118,21 @@ struct StageArgs {
   const void *psi_sw[16];
   void *ring;          // 2 slots x X strings x 2^(n-1) V
   double *slots;       // per warp: 2 (1 + NQ) doubles
-  unsigned *stage;     // [0] stage index, [1] CTAs finished in the current stage
+  unsigned *stage;     // [0] stage index of node 0 of the current graph replay
   uint64_t k_begin, k_end;
   QParams qp;
   TmaGeom g;
   int n, X, nbatch, tma;
+  int node;            // position of this launch in the captured graph
 };
+
+// wait for the preceding grid (programmatic dependent launch); immediate otherwise
+__device__ __forceinline__ void wait_prior_grid() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+// let the next grid in the stream be scheduled before this one finishes
+__device__ __forceinline__ void allow_next_grid() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+
+// one thread: advance the stage base past the stages of the replay that just ran
+__global__ void k_stage_advance(unsigned *stage, unsigned count);
 
 template <typename T, int R, int HI, int QS>
 __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
@@ -129,7 +143,9 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
   extern __shared__ __align__(1024) unsigned char smem_stage[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   V *sm = reinterpret_cast<V *>(smem_stage) + warp * (32 * R);
-  const long long t = (long long)*(volatile unsigned *)a.stage;
+  allow_next_grid();
+  // the base only changes between replays, after every node of the replay has finished
+  const long long t = (long long)*(volatile unsigned *)a.stage + a.node;
   if (t > a.nbatch) return;  // padding stages of the last graph replay
   const int gwarp = blockIdx.x * SRE_WARPS + warp;
   const int nwarps = gridDim.x * SRE_WARPS;
@@ -144,9 +160,15 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
   dd acc[NQ + 1];
 #pragma unroll
   for (int q = 0; q <= NQ; ++q) acc[q] = dd{0.0, 0.0};
+  // Unit order per warp: one pass-1 unit first (its psi reads and butterflies overlap the
+  // previous stage's tail), then the pass-2 units (they read the previous stage's rows
+  // while those are still in L2), then the other pass-1 units.  Measured on B200 against
+  // pass 1 first / pass 2 first: -5 % to -12 % at n = 18, 20, 21 in FP64.
+  auto pre = [] { wait_prior_grid(); };
+  const long long nfirst = n1 < nwarps ? n1 : nwarps;
   for (long long u = gwarp; u < n1 + n2; u += nwarps) {
-    const bool p2 = u < n2;
-    const long long r = p2 ? u : u - n2;
+    const bool p2 = u >= nfirst && u < nfirst + n2;
+    const long long r = p2 ? u - nfirst : (u < nfirst ? u : u - n2);
     const long long b = p2 ? t - 1 : t;
     const int xs = (int)(r % a.X);
     const uint64_t sub = (uint64_t)(r / a.X);
@@ -162,11 +184,12 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
     if (!p2) {
       const V *src = xi.sw < 0 ? psi : reinterpret_cast<const V *>(a.psi_sw[xi.sw]);
       if (a.tma)
-        p1_unit_tma<R, HI>(src, xi, sub, sm, lane, &a.tmap, a.g, (int)((b & 1) * a.X + xs));
+        p1_unit_tma<R, HI>(src, xi, sub, sm, lane, &a.tmap, a.g, (int)((b & 1) * a.X + xs), pre);
       else
-        p1_unit<R, HI, false>(src, xi, sub, inter_x, sm, lane);
+        p1_unit<R, HI, false>(src, xi, sub, inter_x, sm, lane, pre);
     } else {
       double s[NQ + 1];
+      wait_prior_grid();
       p2_unit<R, HI, QS>(inter_x + (sub << PB), sm, lane, s, a.qp);
       // The tile is dead once read (its slot is rewritten by pass 1 two stages later, in
       // another launch): drop its L2 lines without writing them back to DRAM.
@@ -185,6 +208,7 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
     }
   }
   if (lane == 0 && n2 > 0) {
+    wait_prior_grid();  // the previous stage updates the same slot
     double *sl = a.slots + (size_t)gwarp * 2 * (NQ + 1);
 #pragma unroll
     for (int q = 0; q <= NQ; ++q) {
@@ -194,19 +218,8 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
       sl[2 * q + 1] = v.lo;
     }
   }
-  // the ring rows this warp stored are complete before the stage is reported done
+  // the ring rows this warp stored are complete before the grid ends
   if (a.tma && lane == 0) bulk_wait_all();
-  // the last CTA of the stage advances the stage index for the next launch
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    const unsigned done = atomicAdd(a.stage + 1, 1u);
-    if (done == gridDim.x - 1) {
-      a.stage[1] = 0;
-      a.stage[0] = (unsigned)(t + 1);
-      __threadfence();
-    }
-  }
 }
 
 // ---------------------------------------------------------------------------------

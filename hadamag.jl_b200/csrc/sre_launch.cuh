@@ -12,14 +12,15 @@ namespace hm {
 // captured per CUDA graph.  Every stage costs a fixed few microseconds (launch, the first
 // loads of all warps at once, the tail), which favours large batches, while a ring that
 // outgrows the 126 MB L2 costs DRAM traffic.  Where they pull apart (n >= 18) the default
-// batch comes from `measured_x`, timed on B200 (us per X-string, discarded dead tiles):
-//   FP64  n = 18: X = 32 (0.98; X = 16 1.14)   n = 20: X = 16 (4.38; X = 4 4.75)
-//         n = 21: X = 2  (13.6; X = 8 22.4)
-//   FP32  n = 18: X = 64 (0.52)   n = 20: X = 8 (3.09; X = 16 3.47)   n = 21: X = 8 (10.8)
-// (n = 19 interpolated).  hm_autotune measures and records a batch for the machine at
+// batch comes from `measured_x`, timed on B200 (us per X-string, stage kernels chained
+// by programmatic dependent launch, dead tiles discarded):
+//   FP64  n = 18: X = 32 (0.88)  n = 19: X = 16 (1.83; X = 4 1.94)
+//         n = 20: X = 8 (4.00; X = 16 4.18, X = 4 4.13)  n = 21: X = 2 (10.9; X = 8 22+)
+//   FP32  n = 18: X = 64 (0.49)  n = 19: X = 32 (1.05; X = 16 1.19)
+//         n = 20: X = 8 (2.91; X = 16 4.18)  n = 21: X = 4 (10.9)  hm_autotune measures and records a batch for the machine at
 // hand; setting HM_PARAM_BATCH, _UNITS or _RING switches to the generic rule.
 inline int measured_x(bool fp64, int n) {
-  static const int f64[4] = {32, 16, 16, 2}, f32[4] = {64, 16, 8, 8};
+  static const int f64[4] = {32, 16, 8, 2}, f32[4] = {64, 32, 8, 4};
   return (n >= 18 && n <= 21) ? (fp64 ? f64 : f32)[n - 18] : 0;
 }
 
@@ -156,15 +157,38 @@ static int launch_stages(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   HM_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  for (int s = 0; s < G; ++s) kern<<<blocks, SRE_WARPS * 32, smem, c->stream>>>(a);
-  cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
-  if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "stage graph capture failed: %s", cudaGetErrorString(ce));
+  cudaError_t ce = cudaSuccess;
+  for (int s = 0; s < G && ce == cudaSuccess; ++s) {
+    a.node = s;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(blocks);
+    lc.blockDim = dim3(SRE_WARPS * 32);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = at;
+    lc.numAttrs = s > 0 ? 1 : 0;  // node 0 waits for everything before it
+    ce = cudaLaunchKernelEx(&lc, kern, a);
+  }
+  if (ce == cudaSuccess) {
+    k_stage_advance<<<1, 1, 0, c->stream>>>(a.stage, (unsigned)G);
+    ce = cudaGetLastError();
+  }
+  const cudaError_t ce_end = cudaStreamEndCapture(c->stream, &graph);
+  if (ce == cudaSuccess) ce = ce_end;
+  if (ce != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return set_err(c, HM_ERR_CUDA, "stage graph capture failed: %s", cudaGetErrorString(ce));
+  }
   ce = cudaGraphInstantiate(&exec, graph, 0);
   cudaGraphDestroy(graph);
   if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "stage graph instantiation failed: %s", cudaGetErrorString(ce));
   for (int s = 0; s < nst && ce == cudaSuccess; s += G) {
     ce = cudaGraphLaunch(exec, c->stream);
-    c->launches += G;
+    c->launches += G + 1;
   }
   cudaGraphExecDestroy(exec);
   if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "stage graph launch failed: %s", cudaGetErrorString(ce));
