@@ -6,7 +6,8 @@ points per X-string) while the whole run stays short:
 
     python hadamag.jl_b200/prof_case.py --n 20 --k0 1024 --count 256 --precision fp64
 
-Prints the sums and the device time of the call.
+Prints the sums and the device time of the call.  With --grad it runs the adjoint
+(hm_sre_grad, q = 2) on the whole n-qubit state instead.
 """
 import argparse
 import os
@@ -26,11 +27,17 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=sorted(hm.PRECISIONS))
     ap.add_argument("--q", type=float, nargs="+", default=[2.0])
     ap.add_argument("--repeat", type=int, default=2)
+    ap.add_argument("--grad", action="store_true", help="run the adjoint on the whole state")
     args = ap.parse_args()
     g = np.random.default_rng(args.n)
     psi = g.normal(size=1 << args.n) + 1j * g.normal(size=1 << args.n)
     psi /= np.linalg.norm(psi)
     ctx = hm._native.default_context(0)
+    if args.grad:
+        for _ in range(args.repeat):
+            v, g = ctx.sre_grad(psi, args.q[0])
+        print(f"n={args.n} grad: sre={v:.15g} |g|={np.linalg.norm(g):.6g} kernel_ms={ctx.last_kernel_ms():.3f}")
+        return
     for _ in range(args.repeat):
         p2, m = ctx.sre_range(psi, args.k0, args.k0 + args.count, tuple(args.q), hm.PRECISIONS[args.precision])
     print(f"n={args.n} k=[{args.k0},{args.k0 + args.count}) p2={p2.sum():.17g} m={m.sum(axis=1)} "
