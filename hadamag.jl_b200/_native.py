@@ -38,6 +38,7 @@ HM_PARAM_BATCH = 1
 HM_PARAM_RING = 2
 HM_PARAM_UNITS = 3
 HM_PARAM_GRAPH = 4
+HM_PARAM_ADJ_BATCH = 5
 
 
 class ArgumentError(ValueError):
@@ -299,7 +300,7 @@ def _log3_exact(size):
 
 
 def set_param(param, value):
-    """Process-wide tuning knob (HM_PARAM_BATCH / HM_PARAM_RING); 0 restores the default."""
+    """Process-wide tuning knob (HM_PARAM_BATCH, _RING, _UNITS, _GRAPH, _ADJ_BATCH); 0 restores the default."""
     rc = load_library().hm_set_param(int(param), int(value))
     if rc != HM_OK:
         raise ArgumentError(f"hm_set_param({param}, {value}) rejected")

@@ -17,7 +17,7 @@
 #include <math.h>
 
 #include "hm_ctx.h"
-#include "sre_kernels.cuh"
+#include "sre_launch.cuh"
 
 namespace hm {
 
@@ -38,24 +38,57 @@ struct AdjArgs {
   int nx;
 };
 
-__device__ __forceinline__ double powi(double y, int e) {
-  double r = 1.0;
-  for (int i = 0; i < e; ++i) r *= y;
+// y^e for an integer 0 <= e <= 7: binary powering in three branch-free steps, so that
+// the unrolled register sweep keeps its instruction-level parallelism
+__device__ __forceinline__ double powi7(double y, int e) {
+  double r = 1.0, b = y;
+#pragma unroll
+  for (int k = 0; k < 3; ++k) {
+    r = (e & 1) ? r * b : r;
+    b *= b;
+    e >>= 1;
+  }
   return r;
 }
 
-// pointwise map on every register: accumulate sum (W^2)^q, replace W by c W^{2q-1}
-__device__ __forceinline__ double adj_pointwise(double2 (&v)[R], int q, double cq) {
-  double m = 0.0;
+// pointwise map on every register: accumulate sum (W^2)^q, replace W by c W^{2q-1}.
+// Q = 2, 3: compile-time exponent, unrolled over the registers; Q = 0: q at run time
+// (1 <= q <= 8), in a rolled loop over the lane's own slots of the warp's shared buffer
+// (an unrolled sweep of the run-time power spills registers).
+template <int Q>
+__device__ __forceinline__ double adj_pointwise(double2 (&v)[R], int q, double cq, double2 *sm, int lane) {
+  if constexpr (Q == 0) {
 #pragma unroll
-  for (int i = 0; i < R; ++i) {
-    const double a = v[i].x, b = v[i].y;
-    const double a2 = a * a, b2 = b * b;
-    m += powi(a2, q) + powi(b2, q);
-    v[i].x = cq * a * powi(a2, q - 1);
-    v[i].y = cq * b * powi(b2, q - 1);
+    for (int i = 0; i < R; ++i) sm[lane + 32 * i] = v[i];
+    double m = 0.0;
+#pragma unroll 1
+    for (int i = 0; i < R; ++i) {
+      double2 w = sm[lane + 32 * i];
+      const double a2 = w.x * w.x, b2 = w.y * w.y;
+      const double pa = powi7(a2, q - 1), pb = powi7(b2, q - 1);
+      m += pa * a2 + pb * b2;
+      w.x = cq * w.x * pa;
+      w.y = cq * w.y * pb;
+      sm[lane + 32 * i] = w;
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) v[i] = sm[lane + 32 * i];
+    __syncwarp();  // the buffer is rewritten by the next transpose
+    return m;
+  } else {
+    double m0 = 0.0, m1 = 0.0;
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const double a = v[i].x, b = v[i].y;
+      const double a2 = a * a, b2 = b * b;
+      const double pa = Q == 2 ? a2 : a2 * a2, pb = Q == 2 ? b2 : b2 * b2;  // (W^2)^(q-1)
+      m0 += pa * a2;
+      m1 += pb * b2;
+      v[i].x = cq * a * pa;
+      v[i].y = cq * b * pb;
+    }
+    return m0 + m1;
   }
-  return m;
 }
 
 // layout B -> layout A (inverse of transpose_ab)
@@ -118,7 +151,7 @@ __global__ void __launch_bounds__(128) k_adj_fused(AdjArgs a) {
     transpose_ab<R>(v, sm, lane);
     reg_wht<R, 0, (NB < 5 ? NB : 5)>(v);
     const int qi = (int)a.q;
-    mloc = adj_pointwise(v, qi, xz ? a.cq_0 : a.cq_x) * (xz ? 1.0 : pow_q_dev(4.0, a.q));
+    mloc = adj_pointwise<0>(v, qi, xz ? a.cq_0 : a.cq_x, sm, lane) * (xz ? 1.0 : pow_q_dev(4.0, a.q));
     reg_wht<R, 0, (NB < 5 ? NB : 5)>(v);
     transpose_ba(v, sm, lane);
     if constexpr (NB > 5) reg_wht<R, 0, NB - 5>(v);
@@ -206,7 +239,7 @@ __global__ void __launch_bounds__(128) k_adj_p2(AdjArgs a) {
       transpose_ab<R>(v, sm, lane);
       reg_wht<R, LOGC, 5>(v);
     }
-    mloc = adj_pointwise(v, (int)a.q, xz ? a.cq_0 : a.cq_x) * (xz ? 1.0 : pow_q_dev(4.0, a.q));
+    mloc = adj_pointwise<0>(v, (int)a.q, xz ? a.cq_0 : a.cq_x, sm, lane) * (xz ? 1.0 : pow_q_dev(4.0, a.q));
     if constexpr (LOGC >= 5) {
       reg_wht<R, LOGC - 5, 5>(v);
     } else {
@@ -318,16 +351,22 @@ __global__ void k_adj_finish(double2 *grad, uint64_t len, const double *mpart, i
 // ---------------------------------------------------------------------------------
 // n >= 12, X-strings x >= 2^PB: stage kernels.  Batch b holds the X consecutive
 // X-strings x_begin + b X + xs (aligned, so they share their pairing bit and the rows
-// rH, sH of every rho; only the low bits xs of x differ).  Stage t runs
-//   gradient units of batch t-3 (row rho, kind A/B, quarter of the row),
-//   forward high + pointwise + backward high of batch t-1 (in place in the ring),
-//   backward low of batch t-2 (Gamma rows, natural element order, into `gam`),
-//   pass 1 of batch t,
-// with the ring in 3 slots and `gam` in 2.  A gradient unit owns its rows and quarter
-// for the whole batch: kind A adds sum_xs conj(Gamma_xs(e)) psi_sH(e ^ xL) to row rH,
-// kind B adds sum_xs Gamma_xs(e) psi_rH(e) to row sH at e ^ xL (gathered at the permuted
-// source positions).  No two units of a stage touch the same gradient entry and each
-// entry's sum runs in a fixed order.
+// rH, sH of every rho; only the low bits xs of x differ).  Stage t runs four kernels,
+// one per kind of unit (independent work inside the stage):
+//   k_adjs_grad  gradient units of batch t-3 (row rho, kind A/B, part of the row),
+//   k_adjs_p1b   backward low of batch t-2 (Gamma rows, natural element order, into `gam`),
+//   k_adjs_p2f   forward high + pointwise + backward high of batch t-1 (in place),
+//   k_adjs_p1    pass 1 of batch t,
+// with the ring in 3 slots and `gam` in 2.  One kernel per kind keeps each kernel's code
+// small: a single kernel holding all four unrolled unit bodies stalled on instruction
+// fetch for more than half of its cycles.  The kernels are chained by programmatic
+// dependent launch; each one waits for its predecessor (and so, transitively, for all
+// earlier kernels: every CTA waits before it exits) before its first access that
+// depends on an earlier stage, and pass 1 runs its psi reads and butterflies before.
+// A gradient unit owns its rows and part for the whole batch: kind A adds
+// sum_xs conj(Gamma_xs(e)) psi_sH(e ^ xL) to row rH, kind B adds
+// sum_xs Gamma_xs(e ^ xL) psi_rH(e ^ xL) to row sH at e.  No two units of a stage
+// touch the same gradient entry and each entry's sum runs in a fixed order.
 constexpr int ADJ_WARPS = 4;
 
 struct AdjStageArgs {
@@ -335,24 +374,34 @@ struct AdjStageArgs {
   double2 *ring;    // 3 slots x X x 2^(n-1), tile-major (pass-1 layout)
   double2 *gam;     // 2 slots x X x 2^(n-1), Gamma rows in natural element order
   double2 *grad;    // 2^n, unscaled dm/dpsi
-  double *mpart;    // per warp: sum of its pointwise-unit moments, over all stages
-  unsigned *stage;  // [0] stage index, [1] CTAs finished in the current stage
+  double2 *gpart;   // (ng - 1) x 2^n partial gradients of X-string groups 1 .. ng-1
+  double *mpart;    // per warp of k_adjs_p2f: sum of its pointwise-unit moments
+  unsigned *stage;  // [0] stage index of node 0 of the current graph replay
   uint64_t x_begin;
   double cq, q4;    // c_q and 4^q for x != 0
   int q, n, X, nbatch;
+  int ng;           // X-string groups per gradient unit row (power of two, divides X)
+  int node;         // stage offset of this launch in the captured graph
 };
 
-// Gradient unit: destination elements p = 32 i + lane, i in [part * GU_REGS, +GU_REGS),
-// of row rH (kind 0) or row sH (kind 1) of batch b.  Every X-string of the batch adds
+__device__ __forceinline__ long long adj_stage_index(const AdjStageArgs &a) {
+  // the base changes only between graph replays, after every node of a replay finished
+  return (long long)*(volatile unsigned *)a.stage + a.node;
+}
+
+// Gradient unit: destination elements p = 32 i + lane, i in [part * GR, +GR), of row rH
+// (kind 0) or row sH (kind 1) of batch b, for the X-strings of group xg (X / ng
+// consecutive ones; group 0 adds into the gradient, group g > 0 into partial buffer
+// g - 1, folded in at the end in group order).  Every X-string of the group adds
 //   kind 0:  conj(Gamma_x(p)) psi(sH, p ^ xL)       (grad at u1 = rH p)
 //   kind 1:  Gamma_x(p ^ xL)  psi(rH, p ^ xL)       (grad at u2 = sH p)
-// gathered at permuted addresses (no shuffles), four X-strings' loads in flight at once,
+// gathered at permuted addresses (no shuffles), GX X-strings' loads in flight at once,
 // summed in the order of xs.
-constexpr int GU_REGS = 4;
-constexpr int GU_PARTS = R / GU_REGS;  // units per row and kind
+constexpr int GR = 1, GX = 8;
+constexpr int GPARTS = R / GR;  // units per row and kind
 
 __device__ __forceinline__ void adj_grad_unit(const AdjStageArgs &a, long long b, uint64_t rho, int kind, int part,
-                                              int lane) {
+                                              int xg, int lane) {
   const uint64_t xlen = 1ull << (a.n - 1);
   const uint64_t xb = a.x_begin + (uint64_t)b * a.X;  // aligned to X: xs occupies the low bits
   const int jt = 63 - __clzll((long long)xb);
@@ -360,20 +409,21 @@ __device__ __forceinline__ void adj_grad_unit(const AdjStageArgs &a, long long b
   const uint32_t xLb = (uint32_t)(xb & ((1u << PB) - 1u));
   const double2 *gam_b = a.gam + (size_t)(b & 1) * a.X * xlen + (rho << PB);
   const double2 *rowA = a.psi + (rH << PB), *rowB = a.psi + (sH << PB);
-  double2 acc[GU_REGS];
+  double2 acc[GR];
 #pragma unroll
-  for (int j = 0; j < GU_REGS; ++j) acc[j] = make_double2(0.0, 0.0);
+  for (int j = 0; j < GR; ++j) acc[j] = make_double2(0.0, 0.0);
+  const int xpg = a.X / a.ng, xs_end = (xg + 1) * xpg;
 #pragma unroll 1
-  for (int xs0 = 0; xs0 < a.X; xs0 += 4) {
-    double2 g[4][GU_REGS], w[4][GU_REGS];
+  for (int xs0 = xg * xpg; xs0 < xs_end; xs0 += GX) {
+    double2 g[GX][GR], w[GX][GR];
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      const int xs = xs0 + u < a.X ? xs0 + u : xs0;  // X < 4: repeat a valid one, masked below
+    for (int u = 0; u < GX; ++u) {
+      const int xs = xs0 + u < xs_end ? xs0 + u : xs0;  // group < GX: repeat a valid one, masked below
       const double2 *g_row = gam_b + (size_t)xs * xlen;
       const uint32_t xL = xLb | (uint32_t)xs;
 #pragma unroll
-      for (int j = 0; j < GU_REGS; ++j) {
-        const uint32_t p = (uint32_t)((part * GU_REGS + j) * 32 + lane);
+      for (int j = 0; j < GR; ++j) {
+        const uint32_t p = (uint32_t)((part * GR + j) * 32 + lane);
         if (kind == 0) {
           g[u][j] = __ldcg(g_row + p);
           w[u][j] = __ldg(rowB + (p ^ xL));
@@ -384,10 +434,10 @@ __device__ __forceinline__ void adj_grad_unit(const AdjStageArgs &a, long long b
       }
     }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-      if (xs0 + u >= a.X) break;
+    for (int u = 0; u < GX; ++u) {
+      if (xs0 + u >= xs_end) break;
 #pragma unroll
-      for (int j = 0; j < GU_REGS; ++j) {
+      for (int j = 0; j < GR; ++j) {
         const double2 gg = g[u][j], ww = w[u][j];
         if (kind == 0) {
           acc[j].x += gg.x * ww.x + gg.y * ww.y;
@@ -399,10 +449,11 @@ __device__ __forceinline__ void adj_grad_unit(const AdjStageArgs &a, long long b
       }
     }
   }
-  double2 *row = a.grad + ((kind == 0 ? rH : sH) << PB);
+  double2 *dst = xg == 0 ? a.grad : a.gpart + ((size_t)(xg - 1) << a.n);
+  double2 *row = dst + ((kind == 0 ? rH : sH) << PB);
 #pragma unroll
-  for (int j = 0; j < GU_REGS; ++j) {
-    const uint32_t p = (uint32_t)((part * GU_REGS + j) * 32 + lane);
+  for (int j = 0; j < GR; ++j) {
+    const uint32_t p = (uint32_t)((part * GR + j) * 32 + lane);
     double2 o = row[p];
     o.x += acc[j].x;
     o.y += acc[j].y;
@@ -410,120 +461,164 @@ __device__ __forceinline__ void adj_grad_unit(const AdjStageArgs &a, long long b
   }
 }
 
+// warps per CTA and CTAs per SM of the gradient kernel (no 32R-register tiles: 16 warps
+// per SM)
+constexpr int GRAD_WARPS = 4, GRAD_CTAS = 4;
+
+__global__ void __launch_bounds__(GRAD_WARPS * 32, GRAD_CTAS) k_adjs_grad(AdjStageArgs a) {
+  const long long t = adj_stage_index(a);
+  allow_next_grid();
+  wait_prior_grid();  // reads Gamma of the previous stage, updates the gradient rows
+  if (t < 3 || t - 3 >= a.nbatch) return;
+  const int lane = threadIdx.x & 31;
+  const int gwarp = blockIdx.x * GRAD_WARPS + (threadIdx.x >> 5), nwarps = gridDim.x * GRAD_WARPS;
+  const long long nu = 2 * GPARTS * (long long)(1ull << (a.n - 1 - PB));
+  for (long long u = gwarp; u < nu * a.ng; u += nwarps) {
+    const long long v = u % nu;
+    adj_grad_unit(a, t - 3, (uint64_t)(v / (2 * GPARTS)), (int)((v / GPARTS) & 1), (int)(v % GPARTS), (int)(u / nu),
+                  lane);
+  }
+}
+
+// grad += gpart[0] + gpart[1] + ... (in group order)
+__global__ void k_adj_fold_groups(double2 *grad, const double2 *gpart, int nparts, uint64_t len) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < len; i += (uint64_t)gridDim.x * blockDim.x) {
+    double2 g = grad[i];
+    for (int k = 0; k < nparts; ++k) {
+      const double2 p = gpart[(size_t)k * len + i];
+      g.x += p.x;
+      g.y += p.y;
+    }
+    grad[i] = g;
+  }
+}
+
+// backward over the low bits of one row of batch t-2; Gamma in natural element order
 template <int HI>
-__global__ void __launch_bounds__(ADJ_WARPS * 32, 2) k_adj_stage(AdjStageArgs a) {
+__global__ void __launch_bounds__(ADJ_WARPS * 32, 2) k_adjs_p1b(AdjStageArgs a) {
   constexpr int LOGC = PB - HI;
   extern __shared__ __align__(16) unsigned char smraw[];
+  const long long t = adj_stage_index(a);
+  allow_next_grid();
+  wait_prior_grid();  // reads the previous stage's forward-high rows, rewrites a Gamma slot
+  if (t < 2 || t - 2 >= a.nbatch) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double2 *sm = reinterpret_cast<double2 *>(smraw) + warp * 32 * R;
-  const long long t = (long long)*(volatile unsigned *)a.stage;
-  if (t > (long long)a.nbatch + 2) return;  // padding stages of the last graph replay
   const int gwarp = blockIdx.x * ADJ_WARPS + warp, nwarps = gridDim.x * ADJ_WARPS;
-  const uint64_t U = 1ull << HI, xlen = 1ull << (a.n - 1);
-  const long long per = (long long)a.X * (long long)U;
-  const long long ng = (t >= 3 && t - 3 < a.nbatch) ? 2 * GU_PARTS * (long long)U : 0;
-  const long long n2 = (t >= 1 && t - 1 < a.nbatch) ? per : 0;
-  const long long nb = (t >= 2 && t - 2 < a.nbatch) ? per : 0;
-  const long long n1 = (t < a.nbatch) ? per : 0;
+  const uint64_t xlen = 1ull << (a.n - 1);
+  const long long per = (long long)a.X << HI, b = t - 2;
+  for (long long r = gwarp; r < per; r += nwarps) {
+    const int xs = (int)(r % a.X);
+    const uint64_t rho = (uint64_t)(r / a.X);
+    const double2 *ring_x = a.ring + ((size_t)(b % 3) * a.X + xs) * xlen;
+    double2 v[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const uint32_t p = (uint32_t)(i * 32 + lane);
+      const uint32_t tt = p >> LOGC, cc = p & ((1u << LOGC) - 1u);
+      v[i] = __ldcg(ring_x + ((size_t)tt << (HI + LOGC)) + (rho << LOGC) + cc);
+    }
+    reg_wht<R, 0, 5>(v);
+    transpose_ba(v, sm, lane);
+    reg_wht<R, 0, 5>(v);  // layout A: register i of lane l holds element 32 i + l
+    double2 *g_row = a.gam + ((size_t)(b & 1) * a.X + xs) * xlen + (rho << PB);
+#pragma unroll
+    for (int i = 0; i < R; ++i) __stcg(g_row + i * 32 + lane, v[i]);
+  }
+}
+
+// forward over the row bits, pointwise map, backward over the row bits (batch t-1, in
+// place in the ring); QA = q for q = 2, 3, else 0 (q at run time)
+template <int HI, int QA>
+__global__ void __launch_bounds__(ADJ_WARPS * 32, 2) k_adjs_p2f(AdjStageArgs a) {
+  constexpr int LOGC = PB - HI;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const long long t = adj_stage_index(a);
+  allow_next_grid();
+  wait_prior_grid();  // reads the previous stage's pass-1 rows; updates the moment slots
+  if (t < 1 || t - 1 >= a.nbatch) return;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2 *sm = reinterpret_cast<double2 *>(smraw) + warp * 32 * R;
+  const int gwarp = blockIdx.x * ADJ_WARPS + warp, nwarps = gridDim.x * ADJ_WARPS;
+  const uint64_t xlen = 1ull << (a.n - 1);
+  const long long per = (long long)a.X << HI, b = t - 1;
   double mloc = 0.0;
-  for (long long u = gwarp; u < ng + n2 + nb + n1; u += nwarps) {
-    if (u < ng) {
-      adj_grad_unit(a, t - 3, (uint64_t)(u / (2 * GU_PARTS)), (int)((u / GU_PARTS) & 1), (int)(u % GU_PARTS), lane);
-      continue;
-    }
-    long long r = u - ng;
-    if (r < n2) {
-      // forward over the row bits, pointwise map, backward over the row bits
-      const long long b = t - 1;
-      const int xs = (int)(r % a.X);
-      const uint64_t tile = (uint64_t)(r / a.X);
-      double2 *tp = a.ring + ((size_t)(b % 3) * a.X + xs) * xlen + (tile << PB);
-      double2 v[R];
+  for (long long r = gwarp; r < per; r += nwarps) {
+    const int xs = (int)(r % a.X);
+    const uint64_t tile = (uint64_t)(r / a.X);
+    double2 *tp = a.ring + ((size_t)(b % 3) * a.X + xs) * xlen + (tile << PB);
+    double2 v[R];
 #pragma unroll
-      for (int i = 0; i < R; ++i) v[i] = __ldcg(tp + i * 32 + lane);
-      if constexpr (LOGC >= 5) {
-        reg_wht<R, LOGC - 5, 5>(v);
-      } else {
-        reg_wht<R, 0, 5>(v);
-        transpose_ab<R>(v, sm, lane);
-        reg_wht<R, LOGC, 5>(v);
-      }
-      mloc += adj_pointwise(v, a.q, a.cq) * a.q4;
-      if constexpr (LOGC >= 5) {
-        reg_wht<R, LOGC - 5, 5>(v);
-      } else {
-        reg_wht<R, LOGC, 5>(v);
-        transpose_ba(v, sm, lane);
-        reg_wht<R, 0, 5>(v);
-      }
-#pragma unroll
-      for (int i = 0; i < R; ++i) __stcg(tp + i * 32 + lane, v[i]);
-      continue;
-    }
-    r -= n2;
-    if (r < nb) {
-      // backward over the low bits of one row; Gamma in natural element order to `gam`
-      const long long b = t - 2;
-      const int xs = (int)(r % a.X);
-      const uint64_t rho = (uint64_t)(r / a.X);
-      const double2 *ring_x = a.ring + ((size_t)(b % 3) * a.X + xs) * xlen;
-      double2 v[R];
-#pragma unroll
-      for (int i = 0; i < R; ++i) {
-        const uint32_t p = (uint32_t)(i * 32 + lane);
-        const uint32_t tt = p >> LOGC, cc = p & ((1u << LOGC) - 1u);
-        v[i] = __ldcg(ring_x + ((size_t)tt << (HI + LOGC)) + (rho << LOGC) + cc);
-      }
+    for (int i = 0; i < R; ++i) v[i] = __ldcg(tp + i * 32 + lane);
+    if constexpr (LOGC >= 5) {
+      reg_wht<R, LOGC - 5, 5>(v);
+    } else {
       reg_wht<R, 0, 5>(v);
+      transpose_ab<R>(v, sm, lane);
+      reg_wht<R, LOGC, 5>(v);
+    }
+    mloc += adj_pointwise<QA>(v, a.q, a.cq, sm, lane) * a.q4;
+    if constexpr (LOGC >= 5) {
+      reg_wht<R, LOGC - 5, 5>(v);
+    } else {
+      reg_wht<R, LOGC, 5>(v);
       transpose_ba(v, sm, lane);
-      reg_wht<R, 0, 5>(v);  // layout A: register i of lane l holds element 32 i + l
-      double2 *g_row = a.gam + ((size_t)(b & 1) * a.X + xs) * xlen + (rho << PB);
+      reg_wht<R, 0, 5>(v);
+    }
 #pragma unroll
-      for (int i = 0; i < R; ++i) __stcg(g_row + i * 32 + lane, v[i]);
-      continue;
-    }
-    r -= nb;
-    {
-      // pass 1 (forward over the low bits) of batch t
-      const int xs = (int)(r % a.X);
-      const uint64_t rho = (uint64_t)(r / a.X);
-      const uint64_t x = a.x_begin + (uint64_t)t * a.X + xs;
-      XInfo xi;
-      xi.active = 1;
-      xi.sw = -1;
-      xi.xt = x;
-      xi.jt = 63 - __clzll((long long)x);
-      p1_unit<R, HI, false>(a.psi, xi, rho, a.ring + ((size_t)(t % 3) * a.X + xs) * xlen, sm, lane);
-    }
+    for (int i = 0; i < R; ++i) __stcg(tp + i * 32 + lane, v[i]);
   }
   mloc = warp_sum(mloc);
   if (lane == 0) a.mpart[gwarp] += mloc;
-  // the last CTA of the stage advances the stage index for the next launch
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    __threadfence();
-    const unsigned done = atomicAdd(a.stage + 1, 1u);
-    if (done == gridDim.x - 1) {
-      a.stage[1] = 0;
-      a.stage[0] = (unsigned)(t + 1);
-      __threadfence();
-    }
+}
+
+// pass 1 (forward over the low bits) of batch t
+template <int HI>
+__global__ void __launch_bounds__(ADJ_WARPS * 32, 2) k_adjs_p1(AdjStageArgs a) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  const long long t = adj_stage_index(a);
+  allow_next_grid();
+  if (t >= a.nbatch) {
+    wait_prior_grid();
+    return;
   }
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double2 *sm = reinterpret_cast<double2 *>(smraw) + warp * 32 * R;
+  const int gwarp = blockIdx.x * ADJ_WARPS + warp, nwarps = gridDim.x * ADJ_WARPS;
+  const uint64_t xlen = 1ull << (a.n - 1);
+  const long long per = (long long)a.X << HI;
+  // the slot is the one that the previous stage's backward-low units read
+  auto pre = [] { wait_prior_grid(); };
+  for (long long r = gwarp; r < per; r += nwarps) {
+    const int xs = (int)(r % a.X);
+    const uint64_t rho = (uint64_t)(r / a.X);
+    const uint64_t x = a.x_begin + (uint64_t)t * a.X + xs;
+    XInfo xi;
+    xi.active = 1;
+    xi.sw = -1;
+    xi.xt = x;
+    xi.jt = 63 - __clzll((long long)x);
+    p1_unit<R, HI, false>(a.psi, xi, rho, a.ring + ((size_t)(t % 3) * a.X + xs) * xlen, sm, lane, pre);
+  }
+  wait_prior_grid();  // every CTA waits before it exits (transitive ordering of the chain)
 }
 
 // moment slots the stage kernels need: one per warp of a full-occupancy grid
 size_t adj_stage_slots(const hm_ctx *c) { return (size_t)c->num_sms * 8 * ADJ_WARPS; }
 
-template <int HI>
+template <int HI, int QA>
 int launch_adj_stages(hm_ctx *c, const AdjStageArgs &a0, int *nwarps_out) {
   AdjStageArgs a = a0;
   const size_t smem = (size_t)ADJ_WARPS * 32 * R * sizeof(double2);
-  auto kern = k_adj_stage<HI>;
-  HM_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int occ = 0;
-  HM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, ADJ_WARPS * 32, smem));
-  if (occ < 1) occ = 1;
-  const int blocks = c->num_sms * occ;
+  HM_CUDA(c, cudaFuncSetAttribute(k_adjs_p1<HI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  HM_CUDA(c, cudaFuncSetAttribute(k_adjs_p2f<HI, QA>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  HM_CUDA(c, cudaFuncSetAttribute(k_adjs_p1b<HI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0, occ_g = 0;
+  HM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_adjs_p2f<HI, QA>, ADJ_WARPS * 32, smem));
+  HM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_g, k_adjs_grad, GRAD_WARPS * 32, 0));
+  occ = std::max(1, std::min(occ, 8));
+  occ_g = std::max(1, occ_g);
+  const int blocks = c->num_sms * occ, blocks_g = c->num_sms * occ_g;
   const int nw = blocks * ADJ_WARPS;
   HM_TRY(ensure_dev(c, (void **)&c->d_ctrl, &c->ctrl_cap, 4 * sizeof(unsigned)));
   HM_CUDA(c, cudaMemsetAsync(c->d_ctrl, 0, 4 * sizeof(unsigned), c->stream));
@@ -533,9 +628,39 @@ int launch_adj_stages(hm_ctx *c, const AdjStageArgs &a0, int *nwarps_out) {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   HM_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  for (int s = 0; s < G; ++s) kern<<<blocks, ADJ_WARPS * 32, smem, c->stream>>>(a);
-  cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
-  if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "adjoint graph capture failed: %s", cudaGetErrorString(ce));
+  cudaError_t ce = cudaSuccess;
+  for (int s = 0; s < G && ce == cudaSuccess; ++s) {
+    a.node = s;
+    for (int kind = 0; kind < 4 && ce == cudaSuccess; ++kind) {
+      cudaLaunchConfig_t lc = {};
+      lc.gridDim = dim3(kind == 0 ? blocks_g : blocks);
+      lc.blockDim = dim3((kind == 0 ? GRAD_WARPS : ADJ_WARPS) * 32);
+      lc.dynamicSmemBytes = kind == 0 ? 0 : smem;
+      lc.stream = c->stream;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+      at[0].val.programmaticStreamSerializationAllowed = 1;
+      lc.attrs = at;
+      lc.numAttrs = (s > 0 || kind > 0) ? 1 : 0;  // the first node waits for everything before it
+      switch (kind) {
+        case 0: ce = cudaLaunchKernelEx(&lc, k_adjs_grad, a); break;
+        case 1: ce = cudaLaunchKernelEx(&lc, k_adjs_p1b<HI>, a); break;
+        case 2: ce = cudaLaunchKernelEx(&lc, k_adjs_p2f<HI, QA>, a); break;
+        default: ce = cudaLaunchKernelEx(&lc, k_adjs_p1<HI>, a); break;
+      }
+    }
+  }
+  if (ce == cudaSuccess) {
+    k_stage_advance<<<1, 1, 0, c->stream>>>(a.stage, (unsigned)G);
+    ce = cudaGetLastError();
+  }
+  const cudaError_t ce_end = cudaStreamEndCapture(c->stream, &graph);
+  if (ce == cudaSuccess) ce = ce_end;
+  if (ce != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return set_err(c, HM_ERR_CUDA, "adjoint graph capture failed: %s", cudaGetErrorString(ce));
+  }
   ce = cudaGraphInstantiate(&exec, graph, 0);
   cudaGraphDestroy(graph);
   if (ce != cudaSuccess)
@@ -562,20 +687,31 @@ int run_adj_stages(hm_ctx *c, const double2 *psi, int n, int q, double2 *grad, d
   // gradient unit walks the batch's X-strings in sequence) with ring + Gamma rows within
   // 2 GiB.  Measured on B200: n = 14 X = 32 -> 128 cut the time 2.4x, n = 18 X = 16 ->
   // 128 by 18 %, although the larger working set leaves L2.
-  uint64_t X = 128;
+  uint64_t X = twopass_cfg().adj_x > 0 ? (uint64_t)twopass_cfg().adj_x : 128;
   while (X > 1 && 5 * X * xlen * sizeof(double2) > ((uint64_t)2 << 30)) X >>= 1;
   if (X > len - a.x_begin) X = len - a.x_begin;
   a.X = (int)X;
   a.nbatch = (int)((len - a.x_begin) / X);
-  HM_TRY(ensure_dev(c, &c->d_aux, &c->aux_cap, 5 * X * xlen * sizeof(double2)));
+  // X-string groups per gradient row: enough units for about four per gradient warp, so
+  // that the chain of dependent loads of one unit (X / ng X-strings) stays short at small
+  // n; at most 8 groups (each adds one partial gradient to write and fold)
+  const long long units = 2LL * GPARTS * (long long)(xlen >> PB);
+  const long long target = 4LL * c->num_sms * GRAD_CTAS * GRAD_WARPS;
+  int ng = 1;
+  while (ng < 8 && (uint64_t)(2 * ng) * GX <= X && units * ng < target) ng *= 2;
+  a.ng = ng;
+  HM_TRY(ensure_dev(c, &c->d_aux, &c->aux_cap, (5 * X * xlen + (size_t)(ng - 1) * len) * sizeof(double2)));
   a.ring = (double2 *)c->d_aux;
   a.gam = a.ring + 3 * X * xlen;
+  a.gpart = a.gam + 2 * X * xlen;
+  if (ng > 1) HM_CUDA(c, cudaMemsetAsync(a.gpart, 0, (size_t)(ng - 1) * len * sizeof(double2), c->stream));
   a.mpart = mpart;  // zeroed by the caller, one slot per warp (adj_stage_slots)
   int r = HM_ERR_SIZE;
   switch (n - 1 - PB) {
-#define HM_ADJS(HIv) \
-  case HIv:          \
-    r = launch_adj_stages<HIv>(c, a, nw); \
+#define HM_ADJS(HIv)                                                                     \
+  case HIv:                                                                              \
+    r = q == 2 ? launch_adj_stages<HIv, 2>(c, a, nw)                                     \
+               : (q == 3 ? launch_adj_stages<HIv, 3>(c, a, nw) : launch_adj_stages<HIv, 0>(c, a, nw)); \
     break;
     HM_ADJS(1)
     HM_ADJS(2)
@@ -590,6 +726,10 @@ int run_adj_stages(hm_ctx *c, const double2 *psi, int n, int q, double2 *grad, d
 #undef HM_ADJS
     default:
       break;
+  }
+  if (r == HM_OK && ng > 1) {
+    k_adj_fold_groups<<<c->num_sms * 4, 256, 0, c->stream>>>(grad, a.gpart, ng - 1, len);
+    HM_CUDA(c, cudaGetLastError());
   }
   return r;
 }

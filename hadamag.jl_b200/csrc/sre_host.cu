@@ -302,6 +302,10 @@ extern "C" int hm_set_param(int param, int value) {
       if (value < 1 || value > 1024) return HM_ERR_ARG;
       cfg.graph_stages = value;
       return HM_OK;
+    case HM_PARAM_ADJ_BATCH:
+      if (value < 0 || value > 4096 || (value & (value - 1))) return HM_ERR_ARG;
+      cfg.adj_x = value;
+      return HM_OK;
     default:
       return HM_ERR_ARG;
   }

@@ -30,6 +30,7 @@ struct TwoPassCfg {
   int units_target = 4096;
   int ring_mib = 64;
   int graph_stages = 32;
+  int adj_x = 0;  // X-strings per batch of the adjoint stage kernels (0: the default rule)
   // batch sizes chosen by hm_autotune, per precision (0 FP64, 1 FP32) and qubit count;
   // 0 = not tuned.  Used when HM_PARAM_BATCH is not set.
   int tuned_x[2][32] = {};

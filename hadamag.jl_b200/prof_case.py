@@ -28,7 +28,9 @@ def main():
     ap.add_argument("--q", type=float, nargs="+", default=[2.0])
     ap.add_argument("--repeat", type=int, default=2)
     ap.add_argument("--grad", action="store_true", help="run the adjoint on the whole state")
+    ap.add_argument("--adj-batch", type=int, default=0, help="X-strings per adjoint stage (0: default)")
     args = ap.parse_args()
+    hm._native.set_param(hm._native.HM_PARAM_ADJ_BATCH, args.adj_batch)
     g = np.random.default_rng(args.n)
     psi = g.normal(size=1 << args.n) + 1j * g.normal(size=1 << args.n)
     psi /= np.linalg.norm(psi)
