@@ -28,6 +28,8 @@ from ._native import (HM_FP32, HM_FP64, HM_PLAIN, PRECISIONS, ArgumentError, Con
 __all__ = [
     "StateVec", "DensityMatrix", "SRE", "MC_SRE", "Mana", "SRE_batched", "SRE_grad", "generate_gray_table",
     "load_state", "reduced_density_matrix", "proposal_stream", "qubits", "qudits", "qudit_dim", "data",
+    "haar_random_unitary", "brick_wall_pairs", "apply_2gate", "apply_2gate_inplace", "apply_brick_wall",
+    "apply_brick_wall_haar", "rand_haar", "rand_cliff",
     "ArgumentError", "HadaMAGError", "Context", "B200",
 ]
 
@@ -291,27 +293,101 @@ def load_state(path, q=2):
     return StateVec(v, q=q)
 
 
-def reduced_density_matrix(psi, NA, side="right", q=None):
-    """rho_A = Tr_B |psi><psi| for a contiguous bipartition (src/DensityMatrix.jl:94-123).
+def reduced_density_matrix(psi, NA, side="right", q=None, device=0):
+    """rho_A = Tr_B |psi><psi| for a contiguous bipartition (src/DensityMatrix.jl:94-123),
+    computed on the GPU (hm_reduced_density_matrix).
 
     side="right" keeps the NA most significant sites, side="left" the NA least
-    significant.  State preparation utility (host numpy), not part of the hot path.
+    significant.
     """
     s = psi if isinstance(psi, StateVec) else StateVec(psi, q=q or 2)
-    qq = s.q
-    if qq not in (2, 3):
+    if s.q not in (2, 3):
         raise ArgumentError("only q=2 and q=3 are implemented")
-    N = s.n
-    if not (0 <= NA <= N):
-        raise ArgumentError(f"need 0 ≤ NA ≤ N (got NA={NA}, N={N})")
-    dimA, dimB = qq ** NA, qq ** (N - NA)
-    v = s.data
-    if side == "left":
-        M = v.reshape(dimB, dimA).T          # M[iA, kB] = psi[iA + dimA kB]
-        rho = M @ M.conj().T
-    elif side == "right":
-        M = v.reshape(dimA, dimB)            # M[iA, kB] = psi[iA dimB + kB]
-        rho = M @ M.conj().T
-    else:
+    if not (0 <= NA <= s.n):
+        raise ArgumentError(f"need 0 ≤ NA ≤ N (got NA={NA}, N={s.n})")
+    if side not in ("left", "right"):
         raise ArgumentError(f"side must be :left or :right (got {side})")
-    return DensityMatrix(rho, q=qq)
+    rho = default_context(device).reduced_density_matrix(s.data, s.q, NA, side)
+    return DensityMatrix(rho, q=s.q)
+
+
+# ----------------------------------------------------------------------------------
+# state preparation on the GPU (src/State.jl:111-374, src/Helpers.jl:102-132)
+
+def haar_random_unitary(q, n_qudits, rng=None):
+    """Haar-random unitary of size q^n x q^n (src/Helpers.jl:102-132): a complex Gaussian
+    matrix, its QR factorisation, and Q with its columns rephased so that diag(R) > 0.
+    Drawn with numpy's Generator; the reference draws from Julia's RNG, so the two
+    streams differ."""
+    if q not in (2, 3):
+        raise ArgumentError("haar_random_unitary: only q=2 and q=3 are implemented")
+    rng = np.random.default_rng() if rng is None else rng
+    N = q ** n_qudits
+    X = rng.normal(size=(N, N)) + 1j * rng.normal(size=(N, N))
+    Q, R = np.linalg.qr(X)
+    d = np.diag(R)
+    ph = np.where(d == 0, 1.0, d / np.where(d == 0, 1.0, np.abs(d)))
+    return Q * ph[None, :]
+
+
+def brick_wall_pairs(n, depth):
+    """Site pairs of a brick-wall circuit in layer order: odd layers (1,2),(3,4),...,
+    even layers (2,3),(4,5),... (src/State.jl:172-178, 212-218)."""
+    return [(s, s + 1) for layer in range(1, depth + 1) for s in range(1 if layer % 2 else 2, n, 2)]
+
+
+def apply_2gate_inplace(sv, gate, s1, s2, device=0):
+    """apply_2gate! (src/State.jl:254-345, 356-364): two-site gate on sites s1, s2
+    (1-based, site 1 least significant), in place, on the GPU."""
+    sv.data[:] = default_context(device).apply_2gate(sv.data, sv.q, gate, s1, s2)
+    return sv
+
+
+def apply_2gate(sv, gate, s1, s2, device=0):
+    """apply_2gate (src/State.jl:366-374): as apply_2gate_inplace on a copy."""
+    return apply_2gate_inplace(StateVec(sv.data.copy(), q=sv.q), gate, s1, s2, device)
+
+
+def apply_brick_wall(sv, depth, gates, device=0):
+    """Brick-wall circuit with the given gates (one per pair of brick_wall_pairs), in
+    place, on the GPU (hm_brick_wall)."""
+    sv.data[:] = default_context(device).brick_wall(sv.data, sv.q, depth, list(gates))
+    return sv
+
+
+def apply_brick_wall_haar(sv, depth, rng=None, device=0):
+    """apply_brick_wall_haar! (src/State.jl:200-236): Haar-random two-site gates in a
+    brick wall, in place."""
+    gates = [haar_random_unitary(sv.q, 2, rng) for _ in brick_wall_pairs(sv.n, depth)]
+    return apply_brick_wall(sv, depth, gates, device)
+
+
+def rand_haar(n, depth, q=2, rng=None, device=0):
+    """rand_haar (src/State.jl:111-124): |0...0> after a depth-`depth` brick wall of
+    Haar-random two-site gates."""
+    if q not in (2, 3):
+        raise ArgumentError("rand_haar: only q=2 (qubits) and q=3 (qutrits) are implemented")
+    v = np.zeros(q ** n, dtype=np.complex128)
+    v[0] = 1.0
+    return apply_brick_wall_haar(StateVec(v, q=q), depth, rng, device)
+
+
+# one-qubit gates (each applied as kron(g, I) on the pair) and CNOT of
+# apply_brick_wall_cliff! (src/State.jl:146-183), as listed there: its "H" entry is the
+# identity matrix and is kept that way
+_CLIFF_ONE = [np.eye(2), np.array([[0, 1], [1, 0]]), np.array([[0, -1j], [1j, 0]]), np.diag([1.0, -1.0]),
+              np.eye(2), np.diag([1.0, 1j])]
+_CLIFF_CNOT = np.array([[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 0, 1], [0, 0, 1, 0]], dtype=np.complex128)
+
+
+def rand_cliff(n, depth=1, rng=None, device=0):
+    """rand_cliff (src/State.jl:126-183): |0...0> after a brick wall whose gates are drawn
+    uniformly from the six one-qubit gates (as kron(g, I)) and CNOT."""
+    rng = np.random.default_rng() if rng is None else rng
+    gates = []
+    for _ in brick_wall_pairs(n, depth):
+        k = int(rng.integers(0, len(_CLIFF_ONE) + 1))
+        gates.append(np.kron(_CLIFF_ONE[k], np.eye(2)) if k < len(_CLIFF_ONE) else _CLIFF_CNOT)
+    v = np.zeros(1 << n, dtype=np.complex128)
+    v[0] = 1.0
+    return apply_brick_wall(StateVec(v, q=2), depth, gates, device)

@@ -33,6 +33,7 @@ EXPORTS = [
     "hm_sre", "hm_sre_dev", "hm_sre_range", "hm_sre_range_dev", "hm_sre_batched", "hm_sre_grad",
     "hm_mc_sre", "hm_mana_pure", "hm_mana_mixed", "hm_gray_table", "hm_gray_table_general", "hm_set_param",
     "hm_last_launch_count", "hm_probe_fp64_peak", "hm_sre_noalloc", "hm_autotune",
+    "hm_apply_2gate", "hm_brick_wall", "hm_reduced_density_matrix",
 ]
 HM_PARAM_BATCH = 1
 HM_PARAM_RING = 2
@@ -94,6 +95,9 @@ def load_library(path=None):
         L.hm_probe_fp64_peak.argtypes = [_vp, _dp]
         L.hm_sre_noalloc.argtypes = [_dp, i, _dp, i, _dp, _dp, _vp]
         L.hm_autotune.argtypes = [_vp, i, i, _ip, _dp]
+        L.hm_apply_2gate.argtypes = [_vp, _dp, i, i, _dp, i, i]
+        L.hm_brick_wall.argtypes = [_vp, _dp, i, i, i, _dp, i]
+        L.hm_reduced_density_matrix.argtypes = [_vp, _dp, i, i, i, i, _dp]
         for name in EXPORTS:
             if name != "hm_last_error" and name != "hm_abi_version":
                 getattr(L, name).restype = i
@@ -273,6 +277,43 @@ class Context:
                                            flips.ctypes.data_as(_i64p)), "hm_gray_table")
         return codes, flips[: N - 1]
 
+    def apply_2gate(self, psi, q, gate, s1, s2):
+        """Two-site gate on sites s1, s2 (1-based); returns the new amplitudes."""
+        a = np.array(psi, dtype=np.complex128, copy=True)
+        n = _logq_exact(a.size, q)
+        g = _gate_colmajor(gate, q)
+        self._check(self.lib.hm_apply_2gate(self.handle, a.view(np.float64).ctypes.data_as(_dp), n, int(q),
+                                            g.view(np.float64).ctypes.data_as(_dp), int(s1), int(s2)),
+                    "hm_apply_2gate")
+        return a
+
+    def brick_wall(self, psi, q, depth, gates):
+        """Brick-wall circuit with one gate per site pair, in layer order."""
+        a = np.array(psi, dtype=np.complex128, copy=True)
+        n = _logq_exact(a.size, q)
+        gs = (np.ascontiguousarray(np.concatenate([_gate_colmajor(g, q) for g in gates])) if len(gates)
+              else np.zeros(1, dtype=np.complex128))
+        self._check(self.lib.hm_brick_wall(self.handle, a.view(np.float64).ctypes.data_as(_dp), n, int(q),
+                                           int(depth), gs.view(np.float64).ctypes.data_as(_dp), len(gates)),
+                    "hm_brick_wall")
+        return a
+
+    def reduced_density_matrix(self, psi, q, NA, side="right"):
+        """rho_A (q^NA x q^NA) of the NA least ("left") or most ("right") significant sites."""
+        a = np.ascontiguousarray(np.asarray(psi, dtype=np.complex128))
+        n = _logq_exact(a.size, q)
+        if side not in ("left", "right"):
+            raise ArgumentError(f"side must be :left or :right (got {side})")
+        if not 0 <= NA <= n:
+            raise ArgumentError(f"need 0 ≤ NA ≤ N (got NA={NA}, N={n})")
+        dimA = q ** NA
+        rho = np.zeros(dimA * dimA, dtype=np.complex128)
+        self._check(self.lib.hm_reduced_density_matrix(self.handle, a.view(np.float64).ctypes.data_as(_dp), n,
+                                                       int(q), int(NA), 0 if side == "left" else 1,
+                                                       rho.view(np.float64).ctypes.data_as(_dp)),
+                    "hm_reduced_density_matrix")
+        return rho.reshape(dimA, dimA, order="F")
+
     def gray_table_general(self, n, q):
         N = q ** n
         xt = np.zeros(max(N * n, 1), dtype=np.int64)
@@ -280,6 +321,25 @@ class Context:
         self._check(self.lib.hm_gray_table_general(self.handle, int(n), int(q), xt.ctypes.data_as(_i64p),
                                                    flips.ctypes.data_as(_i64p)), "hm_gray_table_general")
         return xt[: N * n].reshape(N, n).T.copy(), flips[: N - 1]
+
+
+def _logq_exact(size, q):
+    if q not in (2, 3):
+        raise ArgumentError(f"only q=2 and q=3 are implemented (got q={q})")
+    n, t = 0, 1
+    while t < size:
+        t *= q
+        n += 1
+    if t != size:
+        raise ArgumentError(f"length(psi)={size} is not a power of q={q}")
+    return n
+
+
+def _gate_colmajor(gate, q):
+    g = np.asarray(gate, dtype=np.complex128)
+    if g.shape != (q * q, q * q):
+        raise ArgumentError(f"gate must be of size (q^2 × q^2) = ({q * q}, {q * q}), got {g.shape}")
+    return np.ascontiguousarray(g.T).reshape(-1)  # column-major element order
 
 
 def _log2_exact(size):

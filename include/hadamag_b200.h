@@ -207,6 +207,31 @@ int hm_gray_table(hm_ctx *ctx, int n, uint64_t *codes, int64_t *flips);
  * 1-based digit positions.  2 <= q <= 16, q^n <= 2^26. */
 int hm_gray_table_general(hm_ctx *ctx, int n, int q, int64_t *xtab, int64_t *flips);
 
+/* ---------------------------------------------------------------------------------- */
+/* State preparation (inputs of the SRE and Mana paths)                                 */
+/* ---------------------------------------------------------------------------------- */
+/* States are q^n interleaved complex doubles on the host, q in {2, 3}, 1 <= n <= 30
+ * (q = 2) or 19 (q = 3).  Sites are 1-based with site 1 the least significant digit;
+ * a two-site gate is q^2 x q^2, column-major, interleaved complex, with row / column
+ * index o1 q + o2 / d1 q + d2 (d1 the digit of site s1). */
+
+/* Apply a two-site gate to sites s1 != s2 in place.  Replaces apply_2gate! of
+ * src/State.jl:254-345 (apply_2gate_qubit! 279-309, apply_2gate_qudit! 311-344). */
+int hm_apply_2gate(hm_ctx *ctx, double *psi, int n, int q, const double *gate, int s1, int s2);
+
+/* Brick-wall circuit in place: layers 1..depth, odd layers on sites (1,2),(3,4),...,
+ * even layers on (2,3),(4,5),...; `gates` holds one q^2 x q^2 gate per site pair in
+ * layer order (ngates must equal that count).  Replaces the loop of
+ * apply_brick_wall_haar! (src/State.jl:200-221) and apply_brick_wall_cliff! (146-183);
+ * the caller draws the gates (haar_random_unitary, src/Helpers.jl:102-132). */
+int hm_brick_wall(hm_ctx *ctx, double *psi, int n, int q, int depth, const double *gates, int ngates);
+
+/* Reduced density matrix rho_A = Tr_B |psi><psi| of a contiguous block of NA sites
+ * (0 <= NA <= n, q^NA <= 16384): side 0 keeps sites 1..NA (`:left`), side 1 keeps
+ * sites n-NA+1..n (`:right`).  rho: q^NA x q^NA, column-major, interleaved complex.
+ * Replaces reduced_density_matrix of src/DensityMatrix.jl:94-123. */
+int hm_reduced_density_matrix(hm_ctx *ctx, const double *psi, int n, int q, int NA, int side, double *rho);
+
 #ifdef __cplusplus
 }
 #endif

@@ -854,3 +854,85 @@ int or_sre_grad(const double *psi, int n, double q, int nthreads, double *sre_ou
     sre_prep_free(&s);
     return OR_OK;
 }
+
+/* ------------------------------------------------------------------------- */
+/* State preparation (the step before the path)                                */
+/* ------------------------------------------------------------------------- */
+
+/* apply_2gate! of src/State.jl:254-345 (apply_2gate_qubit! 279-309, apply_2gate_qudit!
+ * 311-344): for every input index i with digits d1 (site s1) and d2 (site s2), sites
+ * 1-based with site 1 the least significant digit, idx_in = d1 q + d2, and for every
+ * output o = o1 q + o2: tmp[base + o1 q^(s1-1) + o2 q^(s2-1)] += gate[o, idx_in] psi[i].
+ * gate: q^2 x q^2 complex, column-major, interleaved (re, im).  psi: q^n complex,
+ * interleaved, updated in place.  q in {2, 3}; s1 != s2 in [1, n]. */
+int or_apply_2gate(double *psi, int n, int q, const double *gate, int s1, int s2) {
+    if ((q != 2 && q != 3) || n < 2 || s1 < 1 || s2 < 1 || s1 > n || s2 > n || s1 == s2) return OR_ERR_ARG;
+    int64_t N = 1;
+    for (int k = 0; k < n; k++) N *= q;
+    int64_t p1 = 1, p2 = 1;
+    for (int k = 1; k < s1; k++) p1 *= q;
+    for (int k = 1; k < s2; k++) p2 *= q;
+    const int q2 = q * q;
+    double *tmp = calloc((size_t)N * 2, sizeof(double));
+    if (!tmp) return OR_ERR_ARG;
+    for (int64_t i = 0; i < N; i++) {
+        const double ar = psi[2 * i], ai = psi[2 * i + 1];
+        const int64_t d1 = (i / p1) % q, d2 = (i / p2) % q;
+        const int64_t idx_in = d1 * q + d2;
+        const int64_t base = i - d1 * p1 - d2 * p2;
+        for (int o = 0; o < q2; o++) {
+            const int64_t j = base + (o / q) * p1 + (o % q) * p2;
+            const double gr = gate[2 * (o + q2 * idx_in)], gi = gate[2 * (o + q2 * idx_in) + 1];
+            tmp[2 * j] += gr * ar - gi * ai;
+            tmp[2 * j + 1] += gr * ai + gi * ar;
+        }
+    }
+    memcpy(psi, tmp, (size_t)N * 2 * sizeof(double));
+    free(tmp);
+    return OR_OK;
+}
+
+/* apply_brick_wall_haar! of src/State.jl:200-221 (and the layer pattern of
+ * apply_brick_wall_cliff!, 146-183) with the gates given: layer l = 1..depth acts on
+ * sites (s, s+1) for s = 1, 3, 5, ... (odd l) or s = 2, 4, ... (even l), s <= n - 1,
+ * taking the next q^2 x q^2 gate of `gates` for every pair. */
+int or_brick_wall(double *psi, int n, int q, int depth, const double *gates, int ngates) {
+    const int q4 = q * q * q * q;
+    int k = 0;
+    for (int layer = 1; layer <= depth; layer++) {
+        for (int s = (layer & 1) ? 1 : 2; s <= n - 1; s += 2) {
+            if (k >= ngates) return OR_ERR_ARG;
+            int rc = or_apply_2gate(psi, n, q, gates + (size_t)2 * q4 * k, s, s + 1);
+            if (rc != OR_OK) return rc;
+            k++;
+        }
+    }
+    return k == ngates ? OR_OK : OR_ERR_ARG;
+}
+
+/* reduced_density_matrix of src/DensityMatrix.jl:94-123 (rho_A = Tr_B |psi><psi|):
+ * side 0 (:left) keeps sites 1..NA,  rho[iA, jA] = sum_kB psi[iA + dimA kB] conj(psi[jA + dimA kB]);
+ * side 1 (:right) keeps sites N-NA+1..N, rho[iA, jA] = sum_kB psi[iA dimB + kB] conj(psi[jA dimB + kB]).
+ * rho: dimA x dimA complex, column-major, interleaved. */
+int or_reduced_density_matrix(const double *psi, int n, int q, int NA, int side, double *rho) {
+    if ((q != 2 && q != 3) || NA < 0 || NA > n || (side != 0 && side != 1)) return OR_ERR_ARG;
+    int64_t dimA = 1, dimB = 1;
+    for (int k = 0; k < NA; k++) dimA *= q;
+    for (int k = 0; k < n - NA; k++) dimB *= q;
+#pragma omp parallel for schedule(static)
+    for (int64_t jA = 0; jA < dimA; jA++) {
+        for (int64_t iA = 0; iA < dimA; iA++) {
+            double sr = 0.0, si = 0.0;
+            for (int64_t kB = 0; kB < dimB; kB++) {
+                const int64_t a = side == 0 ? iA + dimA * kB : iA * dimB + kB;
+                const int64_t b = side == 0 ? jA + dimA * kB : jA * dimB + kB;
+                const double ar = psi[2 * a], ai = psi[2 * a + 1], br = psi[2 * b], bi = psi[2 * b + 1];
+                sr += ar * br + ai * bi;
+                si += ai * br - ar * bi;
+            }
+            rho[2 * (iA + dimA * jA)] = sr;
+            rho[2 * (iA + dimA * jA) + 1] = si;
+        }
+    }
+    return OR_OK;
+}

@@ -56,6 +56,9 @@ def lib():
         L.or_single_qutrit_M.argtypes = [_dp]
         L.or_mana_mixed.argtypes = [_dp, i, _dp, _dp]
         L.or_sre_grad.argtypes = [_dp, i, d, i, _dp, _dp]
+        L.or_apply_2gate.argtypes = [_dp, i, i, _dp, i, i]
+        L.or_brick_wall.argtypes = [_dp, i, i, i, _dp, i]
+        L.or_reduced_density_matrix.argtypes = [_dp, i, i, i, i, _dp]
         _lib = L
     return _lib
 
@@ -229,3 +232,40 @@ def sre_grad(psi, q=2, nthreads=None):
     _check(lib().or_sre_grad(p, n, float(q), nthreads or nthreads_default(), ctypes.byref(s),
                              g.view(np.float64).ctypes.data_as(_dp)), "sre_grad")
     return s.value, g  # g.real = dSRE/dRe psi, g.imag = dSRE/dIm psi
+
+
+def _gate_buf(gate):
+    g = np.asfortranarray(np.asarray(gate, dtype=np.complex128))
+    return np.ascontiguousarray(g.T.reshape(-1))  # column-major element order
+
+
+def apply_2gate(psi, q, gate, s1, s2):
+    """src/State.jl:254-345: returns the state after the two-site gate (sites 1-based)."""
+    a = np.ascontiguousarray(np.asarray(psi, dtype=np.complex128)).copy()
+    n = int(round(np.log(a.size) / np.log(q)))
+    g = _gate_buf(gate)
+    _check(lib().or_apply_2gate(a.view(np.float64).ctypes.data_as(_dp), n, q,
+                                g.view(np.float64).ctypes.data_as(_dp), s1, s2), "or_apply_2gate")
+    return a
+
+
+def brick_wall(psi, q, depth, gates):
+    """src/State.jl:200-221 with the given layer-order gate list."""
+    a = np.ascontiguousarray(np.asarray(psi, dtype=np.complex128)).copy()
+    n = int(round(np.log(a.size) / np.log(q)))
+    gs = np.ascontiguousarray(np.concatenate([_gate_buf(g) for g in gates])) if len(gates) else np.zeros(1, complex)
+    _check(lib().or_brick_wall(a.view(np.float64).ctypes.data_as(_dp), n, q, depth,
+                               gs.view(np.float64).ctypes.data_as(_dp), len(gates)), "or_brick_wall")
+    return a
+
+
+def reduced_density_matrix(psi, q, NA, side="right"):
+    """src/DensityMatrix.jl:94-123; returns the dimA x dimA matrix."""
+    a = np.ascontiguousarray(np.asarray(psi, dtype=np.complex128))
+    n = int(round(np.log(a.size) / np.log(q)))
+    dimA = q ** NA
+    rho = np.zeros(dimA * dimA, dtype=np.complex128)
+    _check(lib().or_reduced_density_matrix(a.view(np.float64).ctypes.data_as(_dp), n, q, NA,
+                                           0 if side == "left" else 1, rho.view(np.float64).ctypes.data_as(_dp)),
+           "or_reduced_density_matrix")
+    return rho.reshape(dimA, dimA, order="F")

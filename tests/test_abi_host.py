@@ -94,17 +94,17 @@ def test_load_state_roundtrip(hm, tmp_path):
         hm.load_state(str(t))
 
 
-def test_reduced_density_matrix(hm):
+def test_oracle_reduced_density_matrix(oracle):
     # src/DensityMatrix.jl:113-117: rho_A[iA, jA] = sum_kB psi[iA dimB + kB] conj(psi[jA dimB + kB])
     psi = rand_state(3 ** 4, 3)
-    rho = hm.reduced_density_matrix(hm.StateVec(psi, q=3), 2, side="right").data
+    rho = oracle.reduced_density_matrix(psi, 3, 2, side="right")
     dimA, dimB = 9, 9
     ref = np.zeros((dimA, dimA), complex)
     for i in range(dimA):
         for j in range(dimA):
             ref[i, j] = sum(psi[i * dimB + k] * np.conj(psi[j * dimB + k]) for k in range(dimB))
     assert np.allclose(rho, ref, atol=1e-15)
-    rho_l = hm.reduced_density_matrix(hm.StateVec(psi, q=3), 2, side="left").data
+    rho_l = oracle.reduced_density_matrix(psi, 3, 2, side="left")
     ref_l = np.zeros((dimA, dimA), complex)
     for i in range(dimA):
         for j in range(dimA):
@@ -121,3 +121,24 @@ def test_proposal_stream(hm):
     pd2, rs2 = hm.proposal_stream(6, 3, 500, seed=123)
     assert np.array_equal(pd, pd2) and np.array_equal(rs, rs2)
     assert not np.array_equal(pd[0], pd[1])
+
+
+def test_state_prep_argument_errors(hm):
+    # host-side validation; no device work is reached
+    with pytest.raises(hm.ArgumentError):
+        hm.rand_haar(3, 2, q=4)
+    with pytest.raises(hm.ArgumentError):
+        hm.haar_random_unitary(5, 2)
+    with pytest.raises(hm.ArgumentError):
+        hm.reduced_density_matrix(hm.StateVec(rand_state(8, 1)), 4)
+    with pytest.raises(hm.ArgumentError):
+        hm.reduced_density_matrix(hm.StateVec(rand_state(8, 1)), 1, side="middle")
+    assert hm.brick_wall_pairs(5, 3) == [(1, 2), (3, 4), (2, 3), (4, 5), (1, 2), (3, 4)]
+
+
+def test_haar_random_unitary_is_unitary(hm):
+    rng = np.random.default_rng(5)
+    for q in (2, 3):
+        U = hm.haar_random_unitary(q, 2, rng)
+        assert U.shape == (q * q, q * q)
+        assert np.allclose(U.conj().T @ U, np.eye(q * q), atol=1e-13)

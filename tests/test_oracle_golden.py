@@ -159,3 +159,52 @@ def test_grad_matches_finite_differences(oracle):
             fd = (oracle.sre(p, 2)[0] - oracle.sre(m, 2)[0]) / (2 * h)
             an = g[r].real if comp == 1.0 else g[r].imag
             assert an == pytest.approx(fd, rel=1e-5, abs=1e-8)
+
+
+def _apply_2gate_numpy(psi, q, gate, s1, s2):
+    """Independent restatement of apply_2gate! (src/State.jl:279-344) by tensor
+    contraction: site s is axis n - s of the C-order reshaped state."""
+    n = int(round(np.log(psi.size) / np.log(q)))
+    t = psi.reshape((q,) * n)
+    a1, a2 = n - s1, n - s2
+    g = np.asarray(gate).reshape(q, q, q, q)  # [o1, o2, d1, d2]
+    t = np.moveaxis(t, (a1, a2), (0, 1))
+    t = np.einsum("abcd,cd...->ab...", g, t)
+    return np.moveaxis(t, (0, 1), (a1, a2)).reshape(-1)
+
+
+@pytest.mark.parametrize("q,n", [(2, 2), (2, 5), (3, 2), (3, 4)])
+def test_oracle_apply_2gate(oracle, q, n):
+    rng = np.random.default_rng(10 * q + n)
+    psi = rand_state(q ** n, 3 + n)
+    for s1 in range(1, n + 1):
+        for s2 in range(1, n + 1):
+            if s1 == s2:
+                continue
+            gate = rng.normal(size=(q * q, q * q)) + 1j * rng.normal(size=(q * q, q * q))
+            out = oracle.apply_2gate(psi, q, gate, s1, s2)
+            assert np.allclose(out, _apply_2gate_numpy(psi, q, gate, s1, s2), atol=1e-12)
+
+
+def test_oracle_apply_2gate_known_answers(oracle):
+    # CNOT with control site s1 and target s2 (row/column index b1 * 2 + b2)
+    cnot = np.array([[1, 0, 0, 0], [0, 1, 0, 0], [0, 0, 0, 1], [0, 0, 1, 0]], dtype=complex)
+    n = 4
+    for i in range(1 << n):
+        e = np.zeros(1 << n, complex)
+        e[i] = 1
+        out = oracle.apply_2gate(e, 2, cnot, 3, 1)  # control site 3 (bit 2), target site 1 (bit 0)
+        j = i ^ 1 if (i >> 2) & 1 else i
+        assert out[j] == 1 and np.count_nonzero(out) == 1
+
+
+def test_oracle_brick_wall_is_gate_sequence(oracle):
+    rng = np.random.default_rng(3)
+    for q, n, depth in [(2, 5, 3), (3, 4, 2)]:
+        pairs = [(s, s + 1) for layer in range(1, depth + 1) for s in range(1 if layer % 2 else 2, n, 2)]
+        gates = [rng.normal(size=(q * q, q * q)) + 1j * rng.normal(size=(q * q, q * q)) for _ in pairs]
+        psi = rand_state(q ** n, 9)
+        ref = psi.copy()
+        for (s1, s2), g in zip(pairs, gates):
+            ref = _apply_2gate_numpy(ref, q, g, s1, s2)
+        assert np.allclose(oracle.brick_wall(psi, q, depth, gates), ref, atol=1e-10)
