@@ -167,6 +167,64 @@ function ChainRulesCore.rrule(::typeof(sre_value), v::AbstractVector{ComplexF64}
     return val[], sre_pullback
 end
 
+"""
+    apply_2gate!(ψ::StateVec{T,q}, gate, s1, s2)
+
+Two-site gate on sites `s1`, `s2` (1-based, site 1 least significant) on the GPU
+(`hm_apply_2gate`), as `HadaMAG.apply_2gate!` (src/State.jl:254-345).
+"""
+function apply_2gate!(ψ::StateVec{T,q}, gate::AbstractMatrix, s1::Int, s2::Int) where {T,q}
+    v = collect(ComplexF64, data(ψ))
+    g = collect(ComplexF64, gate)              # column-major, as Julia stores it
+    rc = ccall((:hm_apply_2gate, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Float64}, Cint, Cint, Ptr{Float64}, Cint, Cint),
+               context(), reinterpret(Float64, v), qudits(ψ), q, reinterpret(Float64, vec(g)), s1, s2)
+    check(rc, "hm_apply_2gate")
+    data(ψ) .= v
+    return ψ
+end
+
+"""
+    apply_brick_wall_haar!(ψ::StateVec{T,q}, depth, rng = Random.GLOBAL_RNG)
+
+Brick wall of Haar-random two-site gates on the GPU (`hm_brick_wall`); the gates are
+drawn on the host with `HadaMAG.haar_random_unitary`, in the reference's layer order
+(src/State.jl:200-221), so a given `rng` yields the reference's circuit.
+"""
+function apply_brick_wall_haar!(ψ::StateVec{T,q}, depth::Int, rng::AbstractRNG = Random.GLOBAL_RNG) where {T,q}
+    n = qudits(ψ)
+    gates = ComplexF64[]
+    ngates = 0
+    for layer = 1:depth, s = (isodd(layer) ? 1 : 2):2:(n-1)
+        append!(gates, vec(ComplexF64.(HadaMAG.haar_random_unitary(q, 2, rng))))
+        ngates += 1
+    end
+    v = collect(ComplexF64, data(ψ))
+    rc = ccall((:hm_brick_wall, LIB[]), Cint, (Ptr{Cvoid}, Ptr{Float64}, Cint, Cint, Cint, Ptr{Float64}, Cint),
+               context(), reinterpret(Float64, v), n, q, depth, reinterpret(Float64, gates), ngates)
+    check(rc, "hm_brick_wall")
+    data(ψ) .= v
+    return ψ
+end
+
+"""
+    reduced_density_matrix(ψ::StateVec{T,q}, NA; side = :right) -> DensityMatrix
+
+ρ_A on the GPU (`hm_reduced_density_matrix`), as `HadaMAG.reduced_density_matrix`
+(src/DensityMatrix.jl:94-123).
+"""
+function reduced_density_matrix(ψ::StateVec{T,q}, NA::Int; side::Symbol = :right) where {T,q}
+    side in (:left, :right) || throw(ArgumentError("side must be :left or :right (got $side)"))
+    v = collect(ComplexF64, data(ψ))
+    dimA = q^NA
+    ρ = Matrix{ComplexF64}(undef, dimA, dimA)
+    rc = ccall((:hm_reduced_density_matrix, LIB[]), Cint,
+               (Ptr{Cvoid}, Ptr{Float64}, Cint, Cint, Cint, Cint, Ptr{Float64}),
+               context(), reinterpret(Float64, v), qudits(ψ), q, NA, side === :left ? 0 : 1,
+               reinterpret(Float64, vec(ρ)))
+    check(rc, "hm_reduced_density_matrix")
+    return DensityMatrix(ρ; q = q)
+end
+
 HadaMAG._choose_backend(b::B200) = b
 HadaMAG._apply_backend(::B200, fsym, args...; kw...) = getfield(HadaMAGB200, fsym)(args...; kw...)
 
