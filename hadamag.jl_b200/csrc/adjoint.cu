@@ -683,12 +683,19 @@ int run_adj_stages(hm_ctx *c, const double2 *psi, int n, int q, double2 *grad, d
   a.cq = 2.0 * q * pow(4.0, q);
   a.q4 = pow(4.0, q);
   a.x_begin = 1u << PB;
-  // Every stage costs a fixed few microseconds, so the batch is large: X <= 128 (a
-  // gradient unit walks the batch's X-strings in sequence) with ring + Gamma rows within
-  // 2 GiB.  Measured on B200: n = 14 X = 32 -> 128 cut the time 2.4x, n = 18 X = 16 ->
-  // 128 by 18 %, although the larger working set leaves L2.
-  uint64_t X = twopass_cfg().adj_x > 0 ? (uint64_t)twopass_cfg().adj_x : 128;
-  while (X > 1 && 5 * X * xlen * sizeof(double2) > ((uint64_t)2 << 30)) X >>= 1;
+  // Batch size: from HM_PARAM_ADJ_BATCH, else measured on B200 (time of hm_sre_grad over
+  // that of hm_sre, q = 2; the stages are fixed-cost, which favours large batches until
+  // the ring + Gamma working set, 5 X 2^(n-1) complex, costs more than it saves):
+  //   n = 14: X = 1024 2.80 (128 .. 512: 3.1)    n = 16: X = 512 2.53 (128: 2.96)
+  //   n = 17: X = 512 2.80 (128: 3.06)           n = 18: X = 512 2.92 (128: 3.12)
+  //   n = 19: X = 128 3.00 (32: 3.08)            n = 20: X = 64 2.90 (32: 2.95, 128: 3.13)
+  //   n = 21: X = 16 4.17 (64: 5.64)
+  // X <= 2^PB keeps every batch aligned inside one pairing-bit class (and divides the
+  // 2^n - 2^PB X-strings); the working set stays within 8 GiB.
+  uint64_t X = twopass_cfg().adj_x > 0 ? (uint64_t)twopass_cfg().adj_x
+                                       : (n <= 15 ? 1024 : n <= 18 ? 512 : n == 19 ? 128 : n == 20 ? 64 : 16);
+  if (X > (1u << PB)) X = 1u << PB;
+  while (X > 1 && 5 * X * xlen * sizeof(double2) > ((uint64_t)8 << 30)) X >>= 1;
   if (X > len - a.x_begin) X = len - a.x_begin;
   a.X = (int)X;
   a.nbatch = (int)((len - a.x_begin) / X);

@@ -303,7 +303,7 @@ extern "C" int hm_set_param(int param, int value) {
       cfg.graph_stages = value;
       return HM_OK;
     case HM_PARAM_ADJ_BATCH:
-      if (value < 0 || value > 4096 || (value & (value - 1))) return HM_ERR_ARG;
+      if (value < 0 || value > 1024 || (value & (value - 1))) return HM_ERR_ARG;
       cfg.adj_x = value;
       return HM_OK;
     default:

@@ -71,7 +71,7 @@ int hm_set_stream(hm_ctx *ctx, void *cuda_stream);
  * intermediate ring in MiB (8..4096; it should stay L2 resident); HM_PARAM_UNITS: warp
  * units per pass the automatic batch size aims for (256..2^20); HM_PARAM_GRAPH: stage
  * kernels captured per CUDA graph (1..1024); HM_PARAM_ADJ_BATCH: X-strings per batch of
- * hm_sre_grad's stage kernels (power of two, 1..4096).  Value 0 restores the default.
+ * hm_sre_grad's stage kernels (power of two, 1..1024).  Value 0 restores the default.
  * Process-wide; returns HM_ERR_ARG for an unknown knob or value. */
 #define HM_PARAM_BATCH 1
 #define HM_PARAM_RING 2

@@ -34,6 +34,7 @@ def test_set_param_validation(hm):
     assert lib.hm_set_param(hm._native.HM_PARAM_BATCH, 4) == 0
     assert lib.hm_set_param(hm._native.HM_PARAM_BATCH, 0) == 0
     assert lib.hm_set_param(hm._native.HM_PARAM_ADJ_BATCH, 48) == hm._native.HM_ERR_ARG
+    assert lib.hm_set_param(hm._native.HM_PARAM_ADJ_BATCH, 2048) == hm._native.HM_ERR_ARG
     assert lib.hm_set_param(hm._native.HM_PARAM_ADJ_BATCH, 64) == 0
     assert lib.hm_set_param(hm._native.HM_PARAM_ADJ_BATCH, 0) == 0
 
