@@ -66,93 +66,130 @@ __device__ __forceinline__ void dft3(double2 &a, double2 &b, double2 &c) {
   c = make_double2(r2, i2);
 }
 
-// H3 over `nd` digits of a set of `nvec` vectors stored at sm[v * vstride + e * estride],
-// e in [0, 3^nd)
-__device__ void h3_smem(double2 *sm, int nd, int nvec, int vstride, int estride) {
-  const int len = ipow3(nd);
-  int step = 1;
-  for (int d = 0; d < nd; ++d) {
-    const int groups = len / 3;  // butterflies per vector per stage
-    for (int t = threadIdx.x; t < nvec * groups; t += blockDim.x) {
-      const int v = t / groups, g = t % groups;
-      const int blk = g / step, off = g % step;
-      const int i0 = blk * 3 * step + off;
-      double2 *base = sm + v * vstride;
-      double2 a = base[i0 * estride], b = base[(i0 + step) * estride], c = base[(i0 + 2 * step) * estride];
-      dft3(a, b, c);
-      base[i0 * estride] = a;
-      base[(i0 + step) * estride] = b;
-      base[(i0 + 2 * step) * estride] = c;
+__host__ __device__ constexpr int ipow3c(int e) { return e <= 0 ? 1 : 3 * ipow3c(e - 1); }
+
+// H3 over the ND digits of `nvec` vectors of 3^ND elements stored at sm[v * VS + e], with
+// compile-time strides (the index arithmetic divides by constants).  Digits go in pairs:
+// one thread loads the 9 elements of a radix-9 group, runs both radix-3 stages in
+// registers and stores them back, so a vector crosses shared memory ceil(ND / 2) times.
+template <int ND, int VS>
+__device__ __forceinline__ void h3_smem(double2 *sm, int nvec) {
+  constexpr int LEN = ipow3c(ND);
+#pragma unroll
+  for (int d = 0; d + 1 < ND; d += 2) {
+    const int step = ipow3c(d);  // constant once the loop is unrolled
+    constexpr int G9 = LEN >= 9 ? LEN / 9 : 1;  // (the loop body only runs when ND >= 2)
+    for (int t = threadIdx.x; t < nvec * G9; t += blockDim.x) {
+      const int v = t / G9, g = t - v * G9;
+      const int blk = g / step, off = g - blk * step;
+      double2 *base = sm + v * VS + blk * 9 * step + off;
+      double2 x[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) x[k] = base[k * step];
+#pragma unroll
+      for (int j = 0; j < 3; ++j) dft3(x[3 * j], x[3 * j + 1], x[3 * j + 2]);  // digit d
+#pragma unroll
+      for (int i = 0; i < 3; ++i) dft3(x[i], x[i + 3], x[i + 6]);  // digit d + 1
+#pragma unroll
+      for (int k = 0; k < 9; ++k) base[k * step] = x[k];
     }
     __syncthreads();
-    step *= 3;
+  }
+  if constexpr (ND % 2 == 1) {
+    constexpr int step = LEN / 3, G3 = LEN / 3;  // the last digit
+    for (int t = threadIdx.x; t < nvec * G3; t += blockDim.x) {
+      const int v = t / G3, off = t - v * G3;
+      double2 *base = sm + v * VS + off;
+      double2 x0 = base[0], x1 = base[step], x2 = base[2 * step];
+      dft3(x0, x1, x2);
+      base[0] = x0;
+      base[step] = x1;
+      base[2 * step] = x2;
+    }
+    __syncthreads();
   }
 }
+
+// shape of the two-pass split for L = LO + HI qutrits: rows of 3^LO elements (pass 1),
+// columns of 3^HI (pass 2), about 2048 elements per CTA
+template <int LO, int HI> struct ManaShape {
+  static constexpr int RL = ipow3c(LO), RH = ipow3c(HI);
+  static constexpr int ROWS = (2048 / RL < 1) ? 1 : (2048 / RL > RH ? RH : 2048 / RL);
+  static constexpr int COLS = (2048 / RH < 1) ? 1 : (2048 / RH > RL ? RL : 2048 / RH);
+};
 
 struct ManaArgs {
   const double2 *psi;
   double2 *inter;  // batch x RH x RL
   double *slots;   // per pass-2 CTA slot: dd (2 doubles)
-  int L, lo, hi, RL, RH, rows_per_cta, cols_per_cta;
-  int x0, nx;  // X-strings of this batch: x0 .. x0 + nx - 1
+  int x0, nx;      // X-strings of this batch: x0 .. x0 + nx - 1
   double invdim;
 };
 
-// pass 1: rows [blockIdx.x * rows_per_cta, ...) of X-string x0 + blockIdx.y
+// pass 1: rows [blockIdx.x * ROWS, ...) of X-string x0 + blockIdx.y
+template <int LO, int HI>
 __global__ void __launch_bounds__(MANA_THREADS) k_mana_p1(ManaArgs a) {
+  using S = ManaShape<LO, HI>;
+  constexpr int RL = S::RL, RH = S::RH, ROWS = S::ROWS;
   extern __shared__ __align__(16) unsigned char smraw[];
   double2 *sm = reinterpret_cast<double2 *>(smraw);
-  int *addL = reinterpret_cast<int *>(sm + a.rows_per_cta * a.RL);
-  int *negL = addL + a.RL;
+  int *addL = reinterpret_cast<int *>(sm + ROWS * RL);
+  int *negL = addL + RL;
+  int *rowA = negL + RL, *rowB = rowA + ROWS;
   const int xi = blockIdx.y;
   if (xi >= a.nx) return;
   const int x = a.x0 + xi;
-  const int xL = x % a.RL, xH = x / a.RL;
-  for (int e = threadIdx.x; e < a.RL; e += blockDim.x) {
-    addL[e] = tadd(e, xL, a.lo);
-    negL[e] = tnegadd(e, xL, a.lo);
+  const int xL = x % RL, xH = x / RL;
+  const int row0 = blockIdx.x * ROWS;
+  const int nrows = min(ROWS, RH - row0);
+  for (int e = threadIdx.x; e < RL; e += blockDim.x) {
+    addL[e] = tadd(e, xL, LO);
+    negL[e] = tnegadd(e, xL, LO);
+  }
+  for (int rr = threadIdx.x; rr < nrows; rr += blockDim.x) {
+    rowA[rr] = tadd(row0 + rr, xH, HI) * RL;
+    rowB[rr] = tnegadd(row0 + rr, xH, HI) * RL;
   }
   __syncthreads();
-  const int row0 = blockIdx.x * a.rows_per_cta;
-  const int nrows = min(a.rows_per_cta, a.RH - row0);
-  for (int t = threadIdx.x; t < nrows * a.RL; t += blockDim.x) {
-    const int rr = t / a.RL, e = t % a.RL;
-    const int rH = row0 + rr;
-    const int cH = tadd(rH, xH, a.hi), dH = tnegadd(rH, xH, a.hi);
-    const double2 p = a.psi[(size_t)cH * a.RL + addL[e]];
-    double2 q = a.psi[(size_t)dH * a.RL + negL[e]];
+  for (int t = threadIdx.x; t < nrows * RL; t += blockDim.x) {
+    const int rr = t / RL, e = t - rr * RL;
+    const double2 p = a.psi[rowA[rr] + addL[e]];
+    double2 q = a.psi[rowB[rr] + negL[e]];
     q.x *= a.invdim;
     q.y *= a.invdim;
-    sm[rr * a.RL + e] = make_double2(p.x * q.x + p.y * q.y, p.x * q.y - p.y * q.x);  // conj(p) * q
+    sm[t] = make_double2(p.x * q.x + p.y * q.y, p.x * q.y - p.y * q.x);  // conj(p) * q
   }
   __syncthreads();
-  h3_smem(sm, a.lo, nrows, a.RL, 1);
-  double2 *out = a.inter + ((size_t)xi * a.RH + row0) * a.RL;
-  for (int t = threadIdx.x; t < nrows * a.RL; t += blockDim.x) out[t] = sm[t];
+  h3_smem<LO, RL>(sm, nrows);
+  double2 *out = a.inter + ((size_t)xi * RH + row0) * RL;
+  for (int t = threadIdx.x; t < nrows * RL; t += blockDim.x) out[t] = sm[t];
 }
 
-// pass 2: columns [blockIdx.x * cols_per_cta, ...) of X-string x0 + blockIdx.y; adds the
-// CTA's sum |W| into its double-double slot
+// pass 2: columns [blockIdx.x * COLS, ...) of X-string x0 + blockIdx.y; adds the CTA's
+// sum |W| into its double-double slot
+template <int LO, int HI>
 __global__ void __launch_bounds__(MANA_THREADS) k_mana_p2(ManaArgs a) {
+  using S = ManaShape<LO, HI>;
+  constexpr int RL = S::RL, RH = S::RH, COLS = S::COLS;
   extern __shared__ __align__(16) unsigned char smraw[];
   double2 *sm = reinterpret_cast<double2 *>(smraw);
   __shared__ double red[MANA_THREADS];
   const int xi = blockIdx.y;
-  const int c0 = blockIdx.x * a.cols_per_cta;
-  const int ncols = min(a.cols_per_cta, a.RL - c0);
-  const double2 *in = a.inter + (size_t)xi * a.RH * a.RL;
+  const int c0 = blockIdx.x * COLS;
+  const int ncols = min(COLS, RL - c0);
+  const double2 *in = a.inter + (size_t)xi * RH * RL;
   if (xi < a.nx) {
     // sm[col * RH + rH]
-    for (int t = threadIdx.x; t < a.RH * ncols; t += blockDim.x) {
-      const int rH = t / ncols, col = t % ncols;
-      sm[col * a.RH + rH] = in[(size_t)rH * a.RL + c0 + col];
+    for (int t = threadIdx.x; t < RH * COLS; t += blockDim.x) {
+      const int rH = t / COLS, col = t - rH * COLS;
+      if (col < ncols) sm[col * RH + rH] = in[(size_t)rH * RL + c0 + col];
     }
   }
   __syncthreads();
-  if (xi < a.nx) h3_smem(sm, a.hi, ncols, a.RH, 1);
+  if (xi < a.nx) h3_smem<HI, RH>(sm, ncols);
   double s = 0.0;
   if (xi < a.nx)
-    for (int t = threadIdx.x; t < a.RH * ncols; t += blockDim.x) s += hypot(sm[t].x, sm[t].y);
+    for (int t = threadIdx.x; t < RH * ncols; t += blockDim.x) s += sqrt(fma(sm[t].x, sm[t].x, sm[t].y * sm[t].y));
   red[threadIdx.x] = s;
   __syncthreads();
   for (int o = blockDim.x / 2; o > 0; o >>= 1) {
@@ -310,41 +347,34 @@ static M9 phase_point_matrix() {
 
 }  // namespace
 
-int run_mana_pure(hm_ctx *c, const double2 *psi, int L, double *sum_dd) {
-  const int D = ipow3(L);
-  const int lo = (L + 1) / 2, hi = L - lo;
+template <int LO, int HI>
+static int run_mana_pure_t(hm_ctx *c, const double2 *psi, double *sum_dd) {
+  using S = ManaShape<LO, HI>;
+  constexpr int D = ipow3c(LO + HI);
   ManaArgs a;
   a.psi = psi;
-  a.L = L;
-  a.lo = lo;
-  a.hi = hi;
-  a.RL = ipow3(lo);
-  a.RH = ipow3(hi);
-  a.rows_per_cta = std::max(1, 2048 / a.RL);
-  if (a.rows_per_cta > a.RH) a.rows_per_cta = a.RH;
-  a.cols_per_cta = std::max(1, std::min(a.RL, 2048 / a.RH));
   a.invdim = 1.0 / (double)D;
   // X-strings per batch: intermediate of at most 32 MiB (L2 resident)
   int B = (int)std::max<size_t>(1, ((size_t)32 << 20) / ((size_t)D * sizeof(double2)));
   if (B > D) B = D;
   HM_TRY(ensure_dev(c, &c->d_inter, &c->inter_cap, (size_t)B * D * sizeof(double2)));
   a.inter = (double2 *)c->d_inter;
-  const int g1 = (a.RH + a.rows_per_cta - 1) / a.rows_per_cta;
-  const int g2 = (a.RL + a.cols_per_cta - 1) / a.cols_per_cta;
+  const int g1 = (S::RH + S::ROWS - 1) / S::ROWS;
+  const int g2 = (S::RL + S::COLS - 1) / S::COLS;
   const size_t nslots = (size_t)g2 * B;
   HM_TRY(ensure_dev(c, (void **)&c->d_partials, &c->partials_cap, nslots * 2 * sizeof(double)));
   HM_CUDA(c, cudaMemsetAsync(c->d_partials, 0, nslots * 2 * sizeof(double), c->stream));
   a.slots = c->d_partials;
-  const size_t sm1 = (size_t)a.rows_per_cta * a.RL * sizeof(double2) + 2 * a.RL * sizeof(int);
-  const size_t sm2 = (size_t)a.cols_per_cta * a.RH * sizeof(double2);
-  HM_CUDA(c, cudaFuncSetAttribute(k_mana_p1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
-  HM_CUDA(c, cudaFuncSetAttribute(k_mana_p2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
+  const size_t sm1 = (size_t)S::ROWS * S::RL * sizeof(double2) + (2 * S::RL + 2 * S::ROWS) * sizeof(int);
+  const size_t sm2 = (size_t)S::COLS * S::RH * sizeof(double2);
+  HM_CUDA(c, cudaFuncSetAttribute(k_mana_p1<LO, HI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
+  HM_CUDA(c, cudaFuncSetAttribute(k_mana_p2<LO, HI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
   HM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
   for (int x0 = 0; x0 < D; x0 += B) {
     a.x0 = x0;
     a.nx = std::min(B, D - x0);
-    k_mana_p1<<<dim3(g1, a.nx), MANA_THREADS, sm1, c->stream>>>(a);
-    k_mana_p2<<<dim3(g2, B), MANA_THREADS, sm2, c->stream>>>(a);
+    k_mana_p1<LO, HI><<<dim3(g1, a.nx), MANA_THREADS, sm1, c->stream>>>(a);
+    k_mana_p2<LO, HI><<<dim3(g2, B), MANA_THREADS, sm2, c->stream>>>(a);
   }
   HM_CUDA(c, cudaGetLastError());
   HM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
@@ -359,6 +389,25 @@ int run_mana_pure(hm_ctx *c, const double2 *psi, int L, double *sum_dd) {
   sum_dd[0] = c->h_out[0];
   sum_dd[1] = c->h_out[1];
   return HM_OK;
+}
+
+int run_mana_pure(hm_ctx *c, const double2 *psi, int L, double *sum_dd) {
+  // rows take the upper half of the digits: lo = ceil(L / 2), hi = L - lo
+  switch (L) {
+    case 1: return run_mana_pure_t<1, 0>(c, psi, sum_dd);
+    case 2: return run_mana_pure_t<1, 1>(c, psi, sum_dd);
+    case 3: return run_mana_pure_t<2, 1>(c, psi, sum_dd);
+    case 4: return run_mana_pure_t<2, 2>(c, psi, sum_dd);
+    case 5: return run_mana_pure_t<3, 2>(c, psi, sum_dd);
+    case 6: return run_mana_pure_t<3, 3>(c, psi, sum_dd);
+    case 7: return run_mana_pure_t<4, 3>(c, psi, sum_dd);
+    case 8: return run_mana_pure_t<4, 4>(c, psi, sum_dd);
+    case 9: return run_mana_pure_t<5, 4>(c, psi, sum_dd);
+    case 10: return run_mana_pure_t<5, 5>(c, psi, sum_dd);
+    case 11: return run_mana_pure_t<6, 5>(c, psi, sum_dd);
+    case 12: return run_mana_pure_t<6, 6>(c, psi, sum_dd);
+    default: return set_err(c, HM_ERR_SIZE, "L = %d qutrits outside [1, 12]", L);
+  }
 }
 
 int run_mana_mixed(hm_ctx *c, const double2 *rho, int N, double *sum_dd) {
