@@ -7,7 +7,8 @@ points per X-string) while the whole run stays short:
     python hadamag.jl_b200/prof_case.py --n 20 --k0 1024 --count 256 --precision fp64
 
 Prints the sums and the device time of the call.  With --grad it runs the adjoint
-(hm_sre_grad, q = 2) on the whole n-qubit state instead.
+(hm_sre_grad, q = 2) on the whole n-qubit state instead; with --mana L, the pure-state
+Mana of a seeded L-qutrit state.
 """
 import argparse
 import os
@@ -29,8 +30,18 @@ def main():
     ap.add_argument("--repeat", type=int, default=2)
     ap.add_argument("--grad", action="store_true", help="run the adjoint on the whole state")
     ap.add_argument("--adj-batch", type=int, default=0, help="X-strings per adjoint stage (0: default)")
+    ap.add_argument("--mana", type=int, default=0, help="run Mana on a seeded L-qutrit state instead")
     args = ap.parse_args()
     hm._native.set_param(hm._native.HM_PARAM_ADJ_BATCH, args.adj_batch)
+    if args.mana:
+        g = np.random.default_rng(args.mana)
+        v = g.normal(size=3 ** args.mana) + 1j * g.normal(size=3 ** args.mana)
+        v /= np.linalg.norm(v)
+        ctx = hm._native.default_context(0)
+        for _ in range(args.repeat):
+            m = ctx.mana_pure(v)
+        print(f"L={args.mana} mana={m:.15g} kernel_ms={ctx.last_kernel_ms():.3f}")
+        return
     g = np.random.default_rng(args.n)
     psi = g.normal(size=1 << args.n) + 1j * g.normal(size=1 << args.n)
     psi /= np.linalg.norm(psi)
