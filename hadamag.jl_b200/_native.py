@@ -33,7 +33,7 @@ EXPORTS = [
     "hm_sre", "hm_sre_dev", "hm_sre_range", "hm_sre_range_dev", "hm_sre_batched", "hm_sre_grad",
     "hm_mc_sre", "hm_mana_pure", "hm_mana_mixed", "hm_gray_table", "hm_gray_table_general", "hm_set_param",
     "hm_last_launch_count", "hm_probe_fp64_peak", "hm_sre_noalloc", "hm_autotune",
-    "hm_apply_2gate", "hm_brick_wall", "hm_reduced_density_matrix",
+    "hm_apply_2gate", "hm_brick_wall", "hm_reduced_density_matrix", "hm_mc_sre_chains", "hm_mana_pure_range",
 ]
 HM_PARAM_BATCH = 1
 HM_PARAM_RING = 2
@@ -95,6 +95,8 @@ def load_library(path=None):
         L.hm_probe_fp64_peak.argtypes = [_vp, _dp]
         L.hm_sre_noalloc.argtypes = [_dp, i, _dp, i, _dp, _dp, _vp]
         L.hm_autotune.argtypes = [_vp, i, i, _ip, _dp]
+        L.hm_mc_sre_chains.argtypes = [_vp, _dp, i, d, i, i, i, i, _u64p, _dp, _dp, _dp, _dp, _u64p]
+        L.hm_mana_pure_range.argtypes = [_vp, _dp, i, ctypes.c_int64, ctypes.c_int64, _dp]
         L.hm_apply_2gate.argtypes = [_vp, _dp, i, i, _dp, i, i]
         L.hm_brick_wall.argtypes = [_vp, _dp, i, i, i, _dp, i]
         L.hm_reduced_density_matrix.argtypes = [_vp, _dp, i, i, i, i, _dp]
@@ -249,7 +251,35 @@ class Context:
                                        fm.ctypes.data_as(_u64p)), "hm_mc_sre")
         return m2.value, M2, M2ADD, P2, fm
 
+    def mc_sre_chains(self, psi, q, nbeta, chain_begin, chain_end, nsamples, prop_delta, rs):
+        """Chains [chain_begin, chain_end) of the nbeta-point beta grid; prop_delta / rs hold
+        those chains' streams.  Returns (M2, M2ADD, P2, final_mask) per chain."""
+        a, p = _cplx(psi)
+        n = _log2_exact(a.size)
+        nch = int(chain_end) - int(chain_begin)
+        pd = np.ascontiguousarray(prop_delta, dtype=np.uint64).reshape(-1)
+        r = _f64(rs).reshape(-1)
+        if nch < 1 or pd.size != nch * nsamples or r.size != nch * nsamples:
+            raise ArgumentError("proposal stream must hold (chain_end - chain_begin) * nsamples entries")
+        M2, M2ADD, P2 = np.zeros(nch), np.zeros(nch), np.zeros(nch)
+        fm = np.zeros(nch, dtype=np.uint64)
+        self._check(self.lib.hm_mc_sre_chains(self.handle, p, n, float(q), int(nbeta), int(chain_begin),
+                                              int(chain_end), int(nsamples), pd.ctypes.data_as(_u64p),
+                                              r.ctypes.data_as(_dp), M2.ctypes.data_as(_dp),
+                                              M2ADD.ctypes.data_as(_dp), P2.ctypes.data_as(_dp),
+                                              fm.ctypes.data_as(_u64p)), "hm_mc_sre_chains")
+        return M2, M2ADD, P2, fm
+
     # ------------------------------------------------------------------ Mana
+    def mana_pure_range(self, psi, x_begin, x_end):
+        """Double-double sum of |W| over the X-strings [x_begin, x_end) (natural order)."""
+        a, p = _cplx(psi)
+        L = _log3_exact(a.size)
+        out = np.zeros(2)
+        self._check(self.lib.hm_mana_pure_range(self.handle, p, L, int(x_begin), int(x_end),
+                                                out.ctypes.data_as(_dp)), "hm_mana_pure_range")
+        return out
+
     def mana_pure(self, psi):
         a, p = _cplx(psi)
         L = _log3_exact(a.size)

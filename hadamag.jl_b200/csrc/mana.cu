@@ -348,7 +348,7 @@ static M9 phase_point_matrix() {
 }  // namespace
 
 template <int LO, int HI>
-static int run_mana_pure_t(hm_ctx *c, const double2 *psi, double *sum_dd) {
+static int run_mana_pure_t(hm_ctx *c, const double2 *psi, int xb, int xe, double *sum_dd) {
   using S = ManaShape<LO, HI>;
   constexpr int D = ipow3c(LO + HI);
   ManaArgs a;
@@ -370,9 +370,9 @@ static int run_mana_pure_t(hm_ctx *c, const double2 *psi, double *sum_dd) {
   HM_CUDA(c, cudaFuncSetAttribute(k_mana_p1<LO, HI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
   HM_CUDA(c, cudaFuncSetAttribute(k_mana_p2<LO, HI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
   HM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
-  for (int x0 = 0; x0 < D; x0 += B) {
+  for (int x0 = xb; x0 < xe; x0 += B) {
     a.x0 = x0;
-    a.nx = std::min(B, D - x0);
+    a.nx = std::min(B, xe - x0);
     k_mana_p1<LO, HI><<<dim3(g1, a.nx), MANA_THREADS, sm1, c->stream>>>(a);
     k_mana_p2<LO, HI><<<dim3(g2, B), MANA_THREADS, sm2, c->stream>>>(a);
   }
@@ -391,21 +391,22 @@ static int run_mana_pure_t(hm_ctx *c, const double2 *psi, double *sum_dd) {
   return HM_OK;
 }
 
-int run_mana_pure(hm_ctx *c, const double2 *psi, int L, double *sum_dd) {
+// sum |W| over the X-strings [xb, xe) (natural order) as a double-double
+int run_mana_pure(hm_ctx *c, const double2 *psi, int L, int xb, int xe, double *sum_dd) {
   // rows take the upper half of the digits: lo = ceil(L / 2), hi = L - lo
   switch (L) {
-    case 1: return run_mana_pure_t<1, 0>(c, psi, sum_dd);
-    case 2: return run_mana_pure_t<1, 1>(c, psi, sum_dd);
-    case 3: return run_mana_pure_t<2, 1>(c, psi, sum_dd);
-    case 4: return run_mana_pure_t<2, 2>(c, psi, sum_dd);
-    case 5: return run_mana_pure_t<3, 2>(c, psi, sum_dd);
-    case 6: return run_mana_pure_t<3, 3>(c, psi, sum_dd);
-    case 7: return run_mana_pure_t<4, 3>(c, psi, sum_dd);
-    case 8: return run_mana_pure_t<4, 4>(c, psi, sum_dd);
-    case 9: return run_mana_pure_t<5, 4>(c, psi, sum_dd);
-    case 10: return run_mana_pure_t<5, 5>(c, psi, sum_dd);
-    case 11: return run_mana_pure_t<6, 5>(c, psi, sum_dd);
-    case 12: return run_mana_pure_t<6, 6>(c, psi, sum_dd);
+    case 1: return run_mana_pure_t<1, 0>(c, psi, xb, xe, sum_dd);
+    case 2: return run_mana_pure_t<1, 1>(c, psi, xb, xe, sum_dd);
+    case 3: return run_mana_pure_t<2, 1>(c, psi, xb, xe, sum_dd);
+    case 4: return run_mana_pure_t<2, 2>(c, psi, xb, xe, sum_dd);
+    case 5: return run_mana_pure_t<3, 2>(c, psi, xb, xe, sum_dd);
+    case 6: return run_mana_pure_t<3, 3>(c, psi, xb, xe, sum_dd);
+    case 7: return run_mana_pure_t<4, 3>(c, psi, xb, xe, sum_dd);
+    case 8: return run_mana_pure_t<4, 4>(c, psi, xb, xe, sum_dd);
+    case 9: return run_mana_pure_t<5, 4>(c, psi, xb, xe, sum_dd);
+    case 10: return run_mana_pure_t<5, 5>(c, psi, xb, xe, sum_dd);
+    case 11: return run_mana_pure_t<6, 5>(c, psi, xb, xe, sum_dd);
+    case 12: return run_mana_pure_t<6, 6>(c, psi, xb, xe, sum_dd);
     default: return set_err(c, HM_ERR_SIZE, "L = %d qutrits outside [1, 12]", L);
   }
 }
@@ -457,9 +458,24 @@ int hm_mana_pure(hm_ctx *c, const double *psi, int L, double *out) {
   HM_TRY(hm::ensure_dev(c, &c->d_psi, &c->psi_cap, D * sizeof(double2)));
   HM_CUDA(c, cudaMemcpyAsync(c->d_psi, psi, D * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
   double s[2];
-  HM_TRY(hm::run_mana_pure(c, (const double2 *)c->d_psi, L, s));
+  HM_TRY(hm::run_mana_pure(c, (const double2 *)c->d_psi, L, 0, (int)D, s));
   *out = log2(s[0] + s[1]) / log2(3.0);
   return HM_OK;
+}
+
+int hm_mana_pure_range(hm_ctx *c, const double *psi, int L, int64_t x_begin, int64_t x_end, double *sum_dd) {
+  if (!c) return HM_ERR_ARG;
+  c->err.clear();
+  if (!psi || !sum_dd) return hm::set_err(c, HM_ERR_ARG, "null pointer");
+  if (L < 1 || L > 12) return hm::set_err(c, HM_ERR_SIZE, "L = %d qutrits outside [1, 12]", L);
+  const int64_t D = hm::ipow3(L);
+  if (x_begin < 0 || x_end > D || x_begin >= x_end)
+    return hm::set_err(c, HM_ERR_ARG, "X-string range [%lld, %lld) outside [0, %lld)", (long long)x_begin,
+                       (long long)x_end, (long long)D);
+  HM_CUDA(c, cudaSetDevice(c->device));
+  HM_TRY(hm::ensure_dev(c, &c->d_psi, &c->psi_cap, (size_t)D * sizeof(double2)));
+  HM_CUDA(c, cudaMemcpyAsync(c->d_psi, psi, (size_t)D * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+  return hm::run_mana_pure(c, (const double2 *)c->d_psi, L, (int)x_begin, (int)x_end, sum_dd);
 }
 
 int hm_mana_mixed(hm_ctx *c, const double *rho, int N, double *out) {

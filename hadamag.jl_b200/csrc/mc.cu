@@ -36,7 +36,8 @@ struct McArgs {
   const double *rs;
   long long *step;  // device step counter
   QParams qp;
-  int n, nbeta, nsamples, U;
+  int n, nbeta, nsamples, U;  // nbeta: chains of this run
+  int chain0, nbeta_grid;     // first chain's index in the beta grid of nbeta_grid points
   double p2_0, m0;  // x = 0 sample
 };
 
@@ -190,7 +191,7 @@ __global__ void k_mc_init(McArgs a) {
     ch.m2 = 0.0;
     ch.p2 = a.p2_0;
     ch.sM2 = ch.sM2sq = ch.sP2 = 0.0;
-    ch.beta = (double)c / (double)(a.nbeta - 1);
+    ch.beta = (double)(a.chain0 + c) / (double)(a.nbeta_grid - 1);
     ch.m_prop = ch.p2_prop = 0.0;
     ch.n = 0;
     a.ch[c] = ch;
@@ -221,6 +222,10 @@ __global__ void k_mc_finish(McArgs a, double *out, uint64_t *final_mask) {
         evena += m2add;
       }
     }
+  }
+  if (a.chain0 != 0 || nb != a.nbeta_grid) {
+    out[0] = 0.0;  // a range of the grid: the caller combines all chains
+    return;
   }
   const double M2_0 = out[1], M2_e = out[1 + 3 * (nb - 1)];
   const double I_res = (h / 3.0) * (M2_0 + M2_e + 4.0 * odd + 2.0 * even);
@@ -291,13 +296,16 @@ int mc_enqueue_step(hm_ctx *c, McArgs &a) {
 
 }  // namespace
 
-int run_mc(hm_ctx *c, const double2 *psi, int n, double q, int nbeta, int nsamples, const uint64_t *pd_dev,
-           const double *rs_dev, double p2_0, double m0, double *out /* 1 + 3 nbeta */, uint64_t *final_mask) {
+int run_mc(hm_ctx *c, const double2 *psi, int n, double q, int nbeta_grid, int chain0, int nbeta, int nsamples,
+           const uint64_t *pd_dev, const double *rs_dev, double p2_0, double m0, double *out /* 1 + 3 nbeta */,
+           uint64_t *final_mask) {
   McArgs a;
   memset(&a, 0, sizeof a);
   a.psi = psi;
   a.n = n;
   a.nbeta = nbeta;
+  a.chain0 = chain0;
+  a.nbeta_grid = nbeta_grid;
   a.nsamples = nsamples;
   a.pd = pd_dev;
   a.rs = rs_dev;
@@ -367,40 +375,71 @@ int run_mc(hm_ctx *c, const double2 *psi, int n, double q, int nbeta, int nsampl
 
 }  // namespace hm
 
+namespace hm {
+namespace {
+
+// chains [cb, ce) of an nbeta-point grid; out: 1 + 3 (ce - cb) doubles
+int mc_chains(hm_ctx *c, const double *psi, int n, double q, int nbeta, int cb, int ce, int nsamples,
+              const uint64_t *prop_delta, const double *rs, double *out, uint64_t *final_mask) {
+  if (!psi || !prop_delta || !rs) return set_err(c, HM_ERR_ARG, "null pointer");
+  if (n < 1 || n > 21) return set_err(c, HM_ERR_SIZE, "MC: n = %d outside [1, 21]", n);
+  if (nbeta < 3 || nbeta % 2 != 1 || nbeta > 32)
+    return set_err(c, HM_ERR_ARG, "Simpson needs an odd number of beta points in [3, 31] (got %d)", nbeta);
+  if (cb < 0 || ce > nbeta || cb >= ce)
+    return set_err(c, HM_ERR_ARG, "chain range [%d, %d) outside the %d-point beta grid", cb, ce, nbeta);
+  if (nsamples < 1) return set_err(c, HM_ERR_ARG, "nsamples must be >= 1");
+  if (!(q >= 1.0 && q <= 16.0)) return set_err(c, HM_ERR_Q, "Renyi index q = %g outside [1, 16]", q);
+  HM_CUDA(c, cudaSetDevice(c->device));
+  const int nch = ce - cb;
+  const size_t len = (size_t)1 << n;
+  const size_t ns = (size_t)nch * nsamples;
+  HM_TRY(ensure_dev(c, &c->d_psi, &c->psi_cap, len * sizeof(double2)));
+  HM_CUDA(c, cudaMemcpyAsync(c->d_psi, psi, len * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+  // m0 and p2_0 of x = 0 (sample_mask!(0), src/SRE.jl:147), before the proposal stream
+  // takes the scratch buffer the plain path uses for its masks
+  QReq qq;
+  qq.nq = 1;
+  qq.q[0] = q;
+  double z[4];
+  HM_TRY(run_sre_plain(c, (const double2 *)c->d_psi, n, 0, 1, qq, z));
+  const double p2_0 = (z[0] + z[1]) / (double)len, m0 = z[2] + z[3];
+  HM_TRY(ensure_dev(c, &c->d_aux, &c->aux_cap, ns * (sizeof(uint64_t) + sizeof(double))));
+  uint64_t *pd = (uint64_t *)c->d_aux;
+  double *r = (double *)(pd + ns);
+  HM_CUDA(c, cudaMemcpyAsync(pd, prop_delta, ns * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
+  HM_CUDA(c, cudaMemcpyAsync(r, rs, ns * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  return run_mc(c, (const double2 *)c->d_psi, n, q, nbeta, cb, nch, nsamples, pd, r, p2_0, m0, out, final_mask);
+}
+
+}  // namespace
+}  // namespace hm
+
 extern "C" int hm_mc_sre(hm_ctx *c, const double *psi, int n, double q, int nbeta, int nsamples,
                          const uint64_t *prop_delta, const double *rs, double *out_m2, double *M2, double *M2ADD,
                          double *P2, uint64_t *final_mask) {
   if (!c) return HM_ERR_ARG;
   c->err.clear();
-  if (!psi || !prop_delta || !rs || !out_m2 || !M2 || !M2ADD || !P2)
-    return hm::set_err(c, HM_ERR_ARG, "null pointer");
-  if (n < 1 || n > 21) return hm::set_err(c, HM_ERR_SIZE, "MC: n = %d outside [1, 21]", n);
-  if (nbeta < 3 || nbeta % 2 != 1 || nbeta > 32)
-    return hm::set_err(c, HM_ERR_ARG, "Simpson needs an odd number of beta points in [3, 31] (got %d)", nbeta);
-  if (nsamples < 1) return hm::set_err(c, HM_ERR_ARG, "nsamples must be >= 1");
-  if (!(q >= 1.0 && q <= 16.0)) return hm::set_err(c, HM_ERR_Q, "Renyi index q = %g outside [1, 16]", q);
-  HM_CUDA(c, cudaSetDevice(c->device));
-  const size_t len = (size_t)1 << n;
-  const size_t ns = (size_t)nbeta * nsamples;
-  HM_TRY(hm::ensure_dev(c, &c->d_psi, &c->psi_cap, len * sizeof(double2)));
-  HM_CUDA(c, cudaMemcpyAsync(c->d_psi, psi, len * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
-  // m0 and p2_0 of x = 0 (sample_mask!(0), src/SRE.jl:147), before the proposal stream
-  // takes the scratch buffer the plain path uses for its masks
-  hm::QReq qq;
-  qq.nq = 1;
-  qq.q[0] = q;
-  double z[4];
-  HM_TRY(hm::run_sre_plain(c, (const double2 *)c->d_psi, n, 0, 1, qq, z));
-  const double p2_0 = (z[0] + z[1]) / (double)len, m0 = z[2] + z[3];
-  HM_TRY(hm::ensure_dev(c, &c->d_aux, &c->aux_cap, ns * (sizeof(uint64_t) + sizeof(double))));
-  uint64_t *pd = (uint64_t *)c->d_aux;
-  double *r = (double *)(pd + ns);
-  HM_CUDA(c, cudaMemcpyAsync(pd, prop_delta, ns * sizeof(uint64_t), cudaMemcpyHostToDevice, c->stream));
-  HM_CUDA(c, cudaMemcpyAsync(r, rs, ns * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  if (!out_m2 || !M2 || !M2ADD || !P2) return hm::set_err(c, HM_ERR_ARG, "null pointer");
   double out[1 + 3 * 32];
-  HM_TRY(hm::run_mc(c, (const double2 *)c->d_psi, n, q, nbeta, nsamples, pd, r, p2_0, m0, out, final_mask));
+  HM_TRY(hm::mc_chains(c, psi, n, q, nbeta, 0, nbeta, nsamples, prop_delta, rs, out, final_mask));
   *out_m2 = out[0];
   for (int i = 0; i < nbeta; ++i) {
+    M2[i] = out[1 + 3 * i];
+    M2ADD[i] = out[2 + 3 * i];
+    P2[i] = out[3 + 3 * i];
+  }
+  return HM_OK;
+}
+
+extern "C" int hm_mc_sre_chains(hm_ctx *c, const double *psi, int n, double q, int nbeta, int chain_begin,
+                                int chain_end, int nsamples, const uint64_t *prop_delta, const double *rs, double *M2,
+                                double *M2ADD, double *P2, uint64_t *final_mask) {
+  if (!c) return HM_ERR_ARG;
+  c->err.clear();
+  if (!M2 || !M2ADD || !P2) return hm::set_err(c, HM_ERR_ARG, "null pointer");
+  double out[1 + 3 * 32];
+  HM_TRY(hm::mc_chains(c, psi, n, q, nbeta, chain_begin, chain_end, nsamples, prop_delta, rs, out, final_mask));
+  for (int i = 0; i < chain_end - chain_begin; ++i) {
     M2[i] = out[1 + 3 * i];
     M2ADD[i] = out[2 + 3 * i];
     P2[i] = out[3 + 3 * i];

@@ -1,4 +1,8 @@
-"""Multi-GPU exact SRE: one process per GPU, the Gray-code range split across ranks.
+"""Multi-GPU runs: one process per GPU.
+
+Exact SRE splits the Gray-code range across ranks; MC_SRE splits its beta chains;
+pure-state Mana splits its ternary X-string range; batched SRE splits its list of
+states by cost.
 
 The reference splits the X-string range over MPI ranks and then over the GPUs of a
 rank (ext/HadaMAGMPICUDAExt.jl:30-106) with HadaMAG.partition_counts
@@ -90,3 +94,124 @@ def sre_sharded(compute_range, n, qs, rank, world, group=None, device=None):
     local = np.concatenate([np.asarray(p2, dtype=np.float64).reshape(2), np.asarray(m, dtype=np.float64).reshape(-1)])
     gathered = allgather_partials(local, group=group, device=device) if world > 1 else local[None, :]
     return combine_partials(gathered, n, len(qs))
+
+
+# ----------------------------------------------------------------------------------
+# padded all_gather of per-rank tables with different row counts
+
+def allgather_rows(rows, max_rows, group=None, device=None, world=1):
+    """all_gather of a (k, w) float64 table, k <= max_rows, padded with NaN; returns the
+    list of each rank's k rows in rank order (one collective of fixed size)."""
+    rows = np.asarray(rows, dtype=np.float64)
+    if rows.ndim == 1:
+        rows = rows[:, None]
+    w = rows.shape[1]
+    buf = np.full((max_rows + 1, w), np.nan)
+    buf[0, 0] = rows.shape[0]  # row 0 carries the count
+    buf[1:1 + rows.shape[0]] = rows
+    g = allgather_partials(buf.reshape(-1), group=group, device=device) if world > 1 else buf.reshape(1, -1)
+    out = []
+    for r in range(g.shape[0]):
+        t = g[r].reshape(max_rows + 1, w)
+        out.append(t[1:1 + int(t[0, 0])])
+    return out
+
+
+# ----------------------------------------------------------------------------------
+# MC_SRE: independent beta chains (src/Backends/Threads.jl:161-221)
+
+def chain_slice(nbeta, rank, world):
+    """[chain_begin, chain_end) of the beta grid owned by `rank`."""
+    counts, displs = partition_counts(nbeta, world)
+    return displs[rank], displs[rank] + counts[rank]
+
+
+def mc_combine(M2, M2ADD):
+    """m2 = -log2(2^-I + I_add) with I, I_add the composite Simpson integrals over the
+    uniform beta grid on [0, 1] (src/Helpers.jl:223-236, src/Backends/Threads.jl:207-220),
+    summed in the same order as hm_mc_sre's device combination."""
+    M2 = np.asarray(M2, dtype=np.float64)
+    M2ADD = np.asarray(M2ADD, dtype=np.float64)
+    nb = M2.size
+    if nb < 3 or nb % 2 != 1:
+        raise ValueError("Simpson needs an odd number of beta points >= 3")
+    h = 1.0 / (nb - 1)
+    odd = even = odda = evena = 0.0
+    for i in range(1, nb - 1):
+        if i % 2 == 1:
+            odd += float(M2[i])
+            odda += float(M2ADD[i])
+        else:
+            even += float(M2[i])
+            evena += float(M2ADD[i])
+    I_res = (h / 3.0) * (float(M2[0]) + float(M2[-1]) + 4.0 * odd + 2.0 * even)
+    I_add = (h / 3.0) * (float(M2ADD[0]) + float(M2ADD[-1]) + 4.0 * odda + 2.0 * evena)
+    return -np.log2(2.0 ** (-I_res) + I_add)
+
+
+def mc_sharded(compute_chains, nbeta, rank, world, group=None, device=None):
+    """MC_SRE over all ranks.  compute_chains(chain_begin, chain_end) -> (M2, M2ADD, P2)
+    for this rank's chains (the C ABI's hm_mc_sre_chains).  Returns
+    (m2, M2[nbeta], M2ADD[nbeta], P2[nbeta]) on every rank."""
+    cb, ce = chain_slice(nbeta, rank, world)
+    if ce > cb:
+        M2, M2ADD, P2 = compute_chains(cb, ce)
+        local = np.stack([np.asarray(M2), np.asarray(M2ADD), np.asarray(P2)], axis=1)
+    else:
+        local = np.zeros((0, 3))
+    per_rank = allgather_rows(local, -(-nbeta // world), group=group, device=device, world=world)
+    allc = np.concatenate(per_rank, axis=0)
+    return mc_combine(allc[:, 0], allc[:, 1]), allc[:, 0], allc[:, 1], allc[:, 2]
+
+
+# ----------------------------------------------------------------------------------
+# Mana of a pure state: X-string range split (src/Backends/Threads.jl:223-271)
+
+def mana_sharded(compute_range, L, rank, world, group=None, device=None):
+    """Mana over all ranks.  compute_range(x_begin, x_end) -> (hi, lo) double-double
+    sum of |W| over this rank's X-strings (the C ABI's hm_mana_pure_range)."""
+    counts, displs = partition_counts(3 ** L, world)
+    xb, xe = displs[rank], displs[rank] + counts[rank]
+    local = np.asarray(compute_range(xb, xe) if xe > xb else (0.0, 0.0), dtype=np.float64).reshape(2)
+    gathered = allgather_partials(local, group=group, device=device) if world > 1 else local[None, :]
+    S = dd_fold(gathered)
+    return np.log2(S[0] + S[1]) / np.log2(3.0)
+
+
+# ----------------------------------------------------------------------------------
+# batched SRE: the list of states split by cost
+
+def balance_states(ns, world):
+    """Deterministic split of states with qubit counts ns over `world` ranks: largest
+    first (4^n work each), each to the least loaded rank (lowest rank on ties).
+    Returns one sorted index list per rank."""
+    order = sorted(range(len(ns)), key=lambda i: (-int(ns[i]), i))
+    load = [0.0] * world
+    parts = [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        parts[r].append(i)
+        load[r] += 4.0 ** int(ns[i])
+    return [sorted(p) for p in parts]
+
+
+def batched_sharded(compute, ns, nq, rank, world, group=None, device=None):
+    """SRE of many states over all ranks.  compute(indices) -> (vals[len, nq], lost[len])
+    for this rank's states (the C ABI's hm_sre_batched).  Returns (vals[S, nq], lost[S])
+    in input order on every rank."""
+    parts = balance_states(ns, world)
+    mine = parts[rank]
+    if mine:
+        vals, lost = compute(mine)
+        local = np.concatenate([np.asarray(vals, dtype=np.float64).reshape(len(mine), nq),
+                                np.asarray(lost, dtype=np.float64).reshape(len(mine), 1)], axis=1)
+    else:
+        local = np.zeros((0, nq + 1))
+    per_rank = allgather_rows(local, max(len(p) for p in parts), group=group, device=device, world=world)
+    vals = np.zeros((len(ns), nq))
+    lost = np.zeros(len(ns))
+    for r, rows in enumerate(per_rank):
+        for j, i in enumerate(parts[r]):
+            vals[i] = rows[j, :nq]
+            lost[i] = rows[j, nq]
+    return vals, lost

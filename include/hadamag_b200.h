@@ -179,6 +179,16 @@ int hm_sre_noalloc(const double *psi, int n, const double *qs, int nq, double *o
 int hm_mc_sre(hm_ctx *ctx, const double *psi, int n, double q, int nbeta, int nsamples, const uint64_t *prop_delta,
               const double *rs, double *out_m2, double *M2, double *M2ADD, double *P2, uint64_t *final_mask);
 
+/* Chains chain_begin .. chain_end-1 of the nbeta-point grid of hm_mc_sre (chain i at
+ * beta_i = i / (nbeta - 1)), for running the chains on several GPUs.  The chains are
+ * independent (src/Backends/Threads.jl:175-205).  prop_delta / rs hold those chains'
+ * streams (nsamples each, in chain order); M2, M2ADD, P2 (and final_mask, optional)
+ * receive chain_end - chain_begin values.  The caller gathers every chain and combines
+ * them with Simpson's rule as hm_mc_sre does (hadamag_b200.shard.mc_sharded). */
+int hm_mc_sre_chains(hm_ctx *ctx, const double *psi, int n, double q, int nbeta, int chain_begin, int chain_end,
+                     int nsamples, const uint64_t *prop_delta, const double *rs, double *M2, double *M2ADD,
+                     double *P2, uint64_t *final_mask);
+
 /* ---------------------------------------------------------------------------------- */
 /* Mana                                                                                 */
 /* ---------------------------------------------------------------------------------- */
@@ -187,6 +197,13 @@ int hm_mc_sre(hm_ctx *ctx, const double *psi, int n, double q, int nbeta, int ns
  * Replaces Mana(psi::StateVec{T,3}) of src/Backends/Threads.jl:223-271 with
  * compute_chunk_mana_qutrits of src/Mana.jl:19-92: log2(sum |W|) / log2(3).  1 <= L <= 12. */
 int hm_mana_pure(hm_ctx *ctx, const double *psi, int L, double *out_mana);
+
+/* Sum of |W| over the ternary X-strings x_begin .. x_end-1 (natural order, 0 <= x_begin <
+ * x_end <= 3^L) as a double-double sum_dd[0] + sum_dd[1].  The sum over every X-string
+ * S gives Mana = log2(S) / log2(3), so ranges can run on several GPUs and be added
+ * (hadamag_b200.shard.mana_sharded; the reference's threads split their X-string range
+ * the same way, src/Backends/Threads.jl:236-262). */
+int hm_mana_pure_range(hm_ctx *ctx, const double *psi, int L, int64_t x_begin, int64_t x_end, double *sum_dd);
 
 /* Mana of an N-qutrit density matrix (3^N x 3^N, column-major, interleaved complex
  * doubles, host).  Replaces Mana(rho::DensityMatrix) of src/Mana.jl:305-314:
