@@ -128,7 +128,7 @@ struct ManaArgs {
 
 // pass 1: rows [blockIdx.x * ROWS, ...) of X-string x0 + blockIdx.y
 template <int LO, int HI>
-__global__ void __launch_bounds__(MANA_THREADS) k_mana_p1(ManaArgs a) {
+__global__ void __launch_bounds__(MANA_THREADS, 4) k_mana_p1(ManaArgs a) {
   using S = ManaShape<LO, HI>;
   constexpr int RL = S::RL, RH = S::RH, ROWS = S::ROWS;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -168,12 +168,12 @@ __global__ void __launch_bounds__(MANA_THREADS) k_mana_p1(ManaArgs a) {
 // pass 2: columns [blockIdx.x * COLS, ...) of X-string x0 + blockIdx.y; adds the CTA's
 // sum |W| into its double-double slot
 template <int LO, int HI>
-__global__ void __launch_bounds__(MANA_THREADS) k_mana_p2(ManaArgs a) {
+__global__ void __launch_bounds__(MANA_THREADS, 4) k_mana_p2(ManaArgs a) {
   using S = ManaShape<LO, HI>;
   constexpr int RL = S::RL, RH = S::RH, COLS = S::COLS;
   extern __shared__ __align__(16) unsigned char smraw[];
   double2 *sm = reinterpret_cast<double2 *>(smraw);
-  __shared__ double red[MANA_THREADS];
+  __shared__ double red[MANA_THREADS / 32];
   const int xi = blockIdx.y;
   const int c0 = blockIdx.x * COLS;
   const int ncols = min(COLS, RL - c0);
@@ -190,16 +190,16 @@ __global__ void __launch_bounds__(MANA_THREADS) k_mana_p2(ManaArgs a) {
   double s = 0.0;
   if (xi < a.nx)
     for (int t = threadIdx.x; t < RH * ncols; t += blockDim.x) s += sqrt(fma(sm[t].x, sm[t].x, sm[t].y * sm[t].y));
-  red[threadIdx.x] = s;
+  // warp sums, then the warps' sums in warp order
+  s = warp_sum(s);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
   __syncthreads();
-  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
-    if (threadIdx.x < o) red[threadIdx.x] += red[threadIdx.x + o];
-    __syncthreads();
-  }
   if (threadIdx.x == 0) {
+    double tot = 0.0;
+    for (int w = 0; w < MANA_THREADS / 32; ++w) tot += red[w];
     double *slot = a.slots + 2 * ((size_t)blockIdx.y * gridDim.x + blockIdx.x);
     dd acc{slot[0], slot[1]};
-    dd_add(acc, red[0]);
+    dd_add(acc, tot);
     slot[0] = acc.hi;
     slot[1] = acc.lo;
   }
