@@ -138,10 +138,13 @@ __global__ void __launch_bounds__(128) k_mc_p2(McArgs a) {
   }
 }
 
-// Metropolis update of every chain (src/SRE.jl:164-186) and next proposal
+// Metropolis update of every chain (src/SRE.jl:164-186) and next proposal.  One warp per
+// chain: for n >= 12 its lanes fold the chain's per-tile partials (lane l takes tiles l,
+// l + 32, ... in double-double, then a fixed butterfly; the order never changes), and
+// lane 0 updates the chain.
 __global__ void k_mc_update(McArgs a, int folded) {
   const long long t = *a.step;
-  const int c = threadIdx.x;
+  const int c = threadIdx.x >> 5, lane = threadIdx.x & 31;
   if (t < a.nsamples && c < a.nbeta) {
     Chain ch = a.ch[c];
     const uint64_t prop = ch.prop;
@@ -149,9 +152,19 @@ __global__ void k_mc_update(McArgs a, int folded) {
     if (prop != 0) {
       if (folded) {
         dd sp{0.0, 0.0}, sm{0.0, 0.0};
-        for (int i = 0; i < a.U; ++i) {
+        for (int i = lane; i < a.U; i += 32) {
           dd_add(sp, a.part[2 * ((size_t)c * a.U + i)]);
           dd_add(sm, a.part[2 * ((size_t)c * a.U + i) + 1]);
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          dd op, om;
+          op.hi = __shfl_xor_sync(0xffffffffu, sp.hi, o);
+          op.lo = __shfl_xor_sync(0xffffffffu, sp.lo, o);
+          om.hi = __shfl_xor_sync(0xffffffffu, sm.hi, o);
+          om.lo = __shfl_xor_sync(0xffffffffu, sm.lo, o);
+          dd_add_dd(sp, op);
+          dd_add_dd(sm, om);
         }
         p2_prop = sp.hi + sp.lo;
         m_prop = sm.hi + sm.lo;
@@ -160,21 +173,23 @@ __global__ void k_mc_update(McArgs a, int folded) {
         m_prop = ch.m_prop;
       }
     }
-    p2_prop /= (double)(1ull << a.n);
-    const double pb = pow(m_prop, ch.beta);
-    const double r = a.rs[(size_t)c * a.nsamples + t];
-    if ((r < pb / ch.prob) && (prop != 0)) {
-      ch.cur = prop;
-      ch.prob = pb;
-      ch.m2 = -log2(m_prop);
-      ch.p2 = p2_prop;
+    if (lane == 0) {
+      p2_prop /= (double)(1ull << a.n);
+      const double pb = pow(m_prop, ch.beta);
+      const double r = a.rs[(size_t)c * a.nsamples + t];
+      if ((r < pb / ch.prob) && (prop != 0)) {
+        ch.cur = prop;
+        ch.prob = pb;
+        ch.m2 = -log2(m_prop);
+        ch.p2 = p2_prop;
+      }
+      ch.sM2 += ch.m2;
+      ch.sM2sq += ch.m2 * ch.m2;
+      ch.sP2 += ch.p2;
+      ch.n += 1;
+      if (t + 1 < a.nsamples) ch.prop = ch.cur ^ a.pd[(size_t)c * a.nsamples + t + 1];
+      a.ch[c] = ch;
     }
-    ch.sM2 += ch.m2;
-    ch.sM2sq += ch.m2 * ch.m2;
-    ch.sP2 += ch.p2;
-    ch.n += 1;
-    if (t + 1 < a.nsamples) ch.prop = ch.cur ^ a.pd[(size_t)c * a.nsamples + t + 1];
-    a.ch[c] = ch;
   }
   __syncthreads();
   if (threadIdx.x == 0 && t < a.nsamples) *a.step = t + 1;
@@ -261,7 +276,7 @@ int mc_enqueue_step(hm_ctx *c, McArgs &a) {
         return set_err(c, HM_ERR_SIZE, "MC: n = %d", n);
     }
 #undef HM_MCF
-    k_mc_update<<<1, 32, 0, c->stream>>>(a, 0);
+    k_mc_update<<<1, 32 * a.nbeta, 0, c->stream>>>(a, 0);
   } else {
     const int hi = n - 11;
     const size_t smem = 4 * 32 * 32 * sizeof(double2);
@@ -289,7 +304,7 @@ int mc_enqueue_step(hm_ctx *c, McArgs &a) {
         return set_err(c, HM_ERR_SIZE, "MC: n = %d outside [1, 21]", n);
     }
 #undef HM_MCP
-    k_mc_update<<<1, 32, 0, c->stream>>>(a, 1);
+    k_mc_update<<<1, 32 * a.nbeta, 0, c->stream>>>(a, 1);
   }
   return HM_OK;
 }
