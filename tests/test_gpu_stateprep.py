@@ -86,3 +86,30 @@ def test_haar_qutrit_pipeline_mana(hm, oracle):
     ref = oracle.reduced_density_matrix(sv.data, 3, 6, "right")
     assert np.max(np.abs(rho.data - ref)) < 1e-13
     assert hm.Mana(rho) == pytest.approx(oracle.mana_mixed(ref), rel=1e-10)
+
+
+def test_state_prep_argument_errors(hm, ctx):
+    psi = rand_state(1 << 4, 1)
+    g = np.eye(4)
+    with pytest.raises(hm.ArgumentError):
+        ctx.apply_2gate(psi, 2, g, 2, 2)  # same site twice
+    with pytest.raises(hm.ArgumentError):
+        ctx.apply_2gate(psi, 2, g, 1, 5)  # site outside [1, n]
+    with pytest.raises(hm.ArgumentError):
+        ctx.apply_2gate(psi, 2, np.eye(9), 1, 2)  # gate of the wrong size
+    with pytest.raises(hm.ArgumentError):
+        ctx.brick_wall(psi, 2, 3, [g] * 3)  # depth 3 on 4 sites takes 5 gates
+    with pytest.raises(hm.ArgumentError):
+        ctx.reduced_density_matrix(psi, 2, 5)
+    with pytest.raises(hm.ArgumentError):
+        ctx.apply_2gate(rand_state(27, 1), 4, np.eye(16), 1, 2)
+    # the state is unchanged by a rejected call, and an identity brick wall is a no-op
+    out = ctx.brick_wall(psi, 2, 3, [g] * 5)
+    assert np.array_equal(out, psi)
+
+
+def test_mana_range_argument_errors(hm, ctx):
+    psi = rand_state(3 ** 4, 2)
+    for a, b in ((0, 0), (5, 3), (-1, 4), (0, 82)):
+        with pytest.raises(hm.ArgumentError):
+            ctx.mana_pure_range(psi, a, b)
