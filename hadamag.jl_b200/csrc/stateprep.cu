@@ -87,29 +87,30 @@ int launch_2gate(hm_ctx *c, double2 *psi, int n, int q, const double *gate_colma
 
 // ---------------------------------------------------------------------------------
 // rho_A[i, j] = sum_k A(i, k) conj(A(j, k)),  A(i, k) = psi[i + dimA k] (left) or
-// psi[i dimB + k] (right); column-major output.  32 x 32 output tiles, 256 threads with
-// 2 x 2 outputs each, k in slices of 16 through shared memory.  blockIdx.z splits k
-// into `nsplit` ranges whose partial tiles are summed afterwards in split order.
-constexpr int RT = 32, RK = 16;
+// psi[i dimB + k] (right); column-major output.  64 x 64 output tiles, 256 threads with
+// 4 x 4 outputs each (16 complex multiply-adds per 8 shared-memory loads), k in slices
+// of 16 through shared memory.  blockIdx.z splits k into `nsplit` ranges whose partial
+// tiles are summed afterwards in split order.
+constexpr int RT = 64, RK = 16;
 
-__global__ void __launch_bounds__(256) k_rdm(const double2 *__restrict__ psi, uint64_t dimA, uint64_t dimB, int side,
+__global__ void __launch_bounds__(256, 2) k_rdm(const double2 *__restrict__ psi, uint64_t dimA, uint64_t dimB, int side,
                                              uint64_t k_per_split, double2 *__restrict__ out) {
   __shared__ double2 As[RT][RK + 1], Bs[RT][RK + 1];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const uint64_t i0 = (uint64_t)blockIdx.x * RT, j0 = (uint64_t)blockIdx.y * RT;
   const uint64_t kb = (uint64_t)blockIdx.z * k_per_split;
   const uint64_t ke = kb + k_per_split < dimB ? kb + k_per_split : dimB;
-  double2 acc[2][2];
+  double2 acc[4][4];
 #pragma unroll
-  for (int a = 0; a < 2; ++a)
+  for (int u = 0; u < 4; ++u)
 #pragma unroll
-    for (int b = 0; b < 2; ++b) acc[a][b] = make_double2(0.0, 0.0);
+    for (int w = 0; w < 4; ++w) acc[u][w] = make_double2(0.0, 0.0);
   for (uint64_t k0 = kb; k0 < ke; k0 += RK) {
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const int e = threadIdx.x + 256 * h;  // element of the 32 x 16 slice
+    for (int h = 0; h < 4; ++h) {
+      const int e = threadIdx.x + 256 * h;  // element of the 64 x 16 slice
       // fast index along consecutive addresses: rows on the left, k on the right
-      const int r = side == 0 ? (e & 31) : (e >> 4), kk = side == 0 ? (e >> 5) : (e & 15);
+      const int r = side == 0 ? (e & 63) : (e >> 4), kk = side == 0 ? (e >> 6) : (e & 15);
       const uint64_t k = k0 + kk;
       const uint64_t ia = i0 + r, ja = j0 + r;
       double2 va = make_double2(0.0, 0.0), vb = make_double2(0.0, 0.0);
@@ -121,18 +122,18 @@ __global__ void __launch_bounds__(256) k_rdm(const double2 *__restrict__ psi, ui
       Bs[r][kk] = vb;
     }
     __syncthreads();
-#pragma unroll 4
+#pragma unroll 2
     for (int kk = 0; kk < RK; ++kk) {
-      double2 a[2], b[2];
+      double2 a[4], b[4];
 #pragma unroll
-      for (int u = 0; u < 2; ++u) {
+      for (int u = 0; u < 4; ++u) {
         a[u] = As[tx + 16 * u][kk];
         b[u] = Bs[ty + 16 * u][kk];
       }
 #pragma unroll
-      for (int u = 0; u < 2; ++u)
+      for (int u = 0; u < 4; ++u)
 #pragma unroll
-        for (int w = 0; w < 2; ++w) {  // a conj(b)
+        for (int w = 0; w < 4; ++w) {  // a conj(b)
           acc[u][w].x = fma(a[u].x, b[w].x, fma(a[u].y, b[w].y, acc[u][w].x));
           acc[u][w].y = fma(a[u].y, b[w].x, fma(-a[u].x, b[w].y, acc[u][w].y));
         }
@@ -141,9 +142,9 @@ __global__ void __launch_bounds__(256) k_rdm(const double2 *__restrict__ psi, ui
   }
   double2 *o = out + (size_t)blockIdx.z * dimA * dimA;
 #pragma unroll
-  for (int u = 0; u < 2; ++u)
+  for (int u = 0; u < 4; ++u)
 #pragma unroll
-    for (int w = 0; w < 2; ++w) {
+    for (int w = 0; w < 4; ++w) {
       const uint64_t i = i0 + tx + 16 * u, j = j0 + ty + 16 * w;
       if (i < dimA && j < dimA) o[i + dimA * j] = acc[u][w];
     }
