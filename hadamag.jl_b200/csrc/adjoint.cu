@@ -689,11 +689,11 @@ int run_adj_stages(hm_ctx *c, const double2 *psi, int n, int q, double2 *grad, d
   //   n = 14: X = 1024 2.80 (128 .. 512: 3.1)    n = 16: X = 512 2.53 (128: 2.96)
   //   n = 17: X = 512 2.80 (128: 3.06)           n = 18: X = 512 2.92 (128: 3.12)
   //   n = 19: X = 128 3.00 (32: 3.08)            n = 20: X = 64 2.90 (32: 2.95, 128: 3.13)
-  //   n = 21: X = 16 4.17 (64: 5.64)
+  //   n = 21: X = 8 3.90 (4: 4.49, 16: 4.17, 64: 5.64)
   // X <= 2^PB keeps every batch aligned inside one pairing-bit class (and divides the
   // 2^n - 2^PB X-strings); the working set stays within 8 GiB.
   uint64_t X = twopass_cfg().adj_x > 0 ? (uint64_t)twopass_cfg().adj_x
-                                       : (n <= 15 ? 1024 : n <= 18 ? 512 : n == 19 ? 128 : n == 20 ? 64 : 16);
+                                       : (n <= 15 ? 1024 : n <= 18 ? 512 : n == 19 ? 128 : n == 20 ? 64 : 8);
   if (X > (1u << PB)) X = 1u << PB;
   while (X > 1 && 5 * X * xlen * sizeof(double2) > ((uint64_t)8 << 30)) X >>= 1;
   if (X > len - a.x_begin) X = len - a.x_begin;
