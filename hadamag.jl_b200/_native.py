@@ -40,6 +40,12 @@ HM_PARAM_RING = 2
 HM_PARAM_UNITS = 3
 HM_PARAM_GRAPH = 4
 HM_PARAM_ADJ_BATCH = 5
+HM_PARAM_ENGINE = 6
+HM_PARAM_QUEUE_SLOTS = 7
+HM_PARAM_QUEUE_SLOT_MIB = 8
+HM_PARAM_QUEUE_CHUNK = 9
+HM_PARAM_QUEUE_CTAS = 10
+HM_PARAM_QUEUE_STALL_TEST = 11
 
 
 class ArgumentError(ValueError):
@@ -390,7 +396,8 @@ def _log3_exact(size):
 
 
 def set_param(param, value):
-    """Process-wide tuning knob (HM_PARAM_BATCH, _RING, _UNITS, _GRAPH, _ADJ_BATCH); 0 restores the default."""
+    """Process-wide tuning knob (HM_PARAM_BATCH, _RING, _UNITS, _GRAPH, _ADJ_BATCH, _ENGINE, _QUEUE_SLOTS,
+    _QUEUE_SLOT_MIB, _QUEUE_CHUNK, _QUEUE_CTAS); 0 restores the default."""
     rc = load_library().hm_set_param(int(param), int(value))
     if rc != HM_OK:
         raise ArgumentError(f"hm_set_param({param}, {value}) rejected")

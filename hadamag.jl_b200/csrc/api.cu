@@ -3,6 +3,9 @@
 #include <math.h>
 #include <stdarg.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "hm_common.cuh"
 #include "hm_ctx.h"
 
@@ -140,7 +143,8 @@ int hm_destroy(hm_ctx *c) {
   if (!c) return HM_ERR_ARG;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
-  void *dev[] = {c->d_psi, c->d_psi32, c->d_inter, c->d_partials, c->d_ctrl, c->d_out, c->d_aux, c->d_aux2};
+  void *dev[] = {c->d_psi, c->d_psi32, c->d_inter, c->d_partials, c->d_ctrl, c->d_out, c->d_aux, c->d_aux2,
+                 c->d_queue};
   for (void *p : dev)
     if (p) cudaFree(p);
   if (c->h_out) cudaFreeHost(c->h_out);
@@ -282,17 +286,47 @@ int hm_sre_batched(hm_ctx *c, int nstates, const double *const *psis, const int 
                                c->stream));
     off += len;
   }
+  // states with n <= 21 go through one persistent queue launch (FP32: plus one FP64
+  // launch of every state's x = 0 transform); larger states and the plain selector run
+  // one state per call
+  c->launches = 0;
+  std::vector<QueueItem> items;
+  std::vector<int> where;
   off = 0;
-  double total_ms = 0.0;
   for (int s = 0; s < nstates; ++s) {
     const size_t len = (size_t)1 << ns[s];
-    double dd[10];
-    HM_TRY(run_sre(c, (const double2 *)c->d_psi + off, ns[s], 0, len, q, precision, dd));
-    total_ms += c->last_ms;
-    sre_finish(dd, ns[s], nq, out_sre + (size_t)s * nq, out_lost + s);
+    if (precision != HM_PLAIN && ns[s] <= 21) {
+      items.push_back(QueueItem{(const double2 *)c->d_psi + off, ns[s], 0, (uint64_t)len});
+      where.push_back(s);
+    }
     off += len;
   }
+  std::vector<double> dd((size_t)nstates * 2 * (1 + nq));
+  double total_ms = 0.0;
+  long long launches = 0;
+  if (!items.empty()) {
+    std::vector<double> qdd(items.size() * 2 * (1 + nq));
+    HM_TRY(run_queue_sre(c, items.data(), (int)items.size(), q, precision, qdd.data()));
+    total_ms += c->last_ms;
+    launches += c->launches;
+    for (size_t i = 0; i < items.size(); ++i)
+      std::copy(qdd.begin() + i * 2 * (1 + nq), qdd.begin() + (i + 1) * 2 * (1 + nq),
+                dd.begin() + (size_t)where[i] * 2 * (1 + nq));
+  }
+  off = 0;
+  for (int s = 0; s < nstates; ++s) {
+    const size_t len = (size_t)1 << ns[s];
+    if (!(precision != HM_PLAIN && ns[s] <= 21)) {
+      c->launches = 0;
+      HM_TRY(run_sre(c, (const double2 *)c->d_psi + off, ns[s], 0, len, q, precision, dd.data() + (size_t)s * 2 * (1 + nq)));
+      total_ms += c->last_ms;
+      launches += c->launches;
+    }
+    off += len;
+  }
+  for (int s = 0; s < nstates; ++s) sre_finish(dd.data() + (size_t)s * 2 * (1 + nq), ns[s], nq, out_sre + (size_t)s * nq, out_lost + s);
   c->last_ms = total_ms;
+  c->launches = launches;
   return HM_OK;
 }
 

@@ -41,6 +41,8 @@ struct hm_ctx {
   size_t h_out_cap = 0;
   void *h_pin = nullptr;  // pinned host scratch
   size_t h_pin_cap = 0;
+  void *d_queue = nullptr;  // queue sweep: state table, batch counters, per-warp slots
+  size_t queue_cap = 0;
 };
 
 namespace hm {
@@ -114,6 +116,36 @@ struct QReq {
   double q[4];
   int nq;
 };
+
+// One state of a queue sweep: a device-resident double2 state and a Gray range.
+struct QueueItem {
+  const double2 *psi;
+  int n;
+  uint64_t kb, ke;
+};
+
+// Tunables of the queue sweep (hm_set_param / hm_autotune): X-strings per ring slot of
+// the largest two-pass state (X, when set; else the tuned table; else a slot of
+// slot_mib MiB), K ring slots, units claimed per atomic, CTAs per SM (0: occupancy).
+struct QueueCfg {
+  int X = 0;
+  int X_set = 0;
+  int slot_mib = 16;
+  int K = 4;
+  int chunk = 1;
+  int ctas_per_sm = 0;
+  int engine = 0;  // single-state sweeps: 0 queue, 1 stage kernels
+  int stall_test = 0;  // test of the bounded waits (HM_PARAM_QUEUE_STALL_TEST)
+  int tuned_x[2][32] = {};
+  int tuned_cps[2][32] = {};
+};
+QueueCfg &queue_cfg();
+
+// Exact-SRE raw sums of several states in one persistent launch (12 <= n <= 21 two-pass
+// states and n <= 11 one-warp states); out_dd per item: [p2_hi, p2_lo, m0_hi, m0_lo, ...].
+int run_queue(hm_ctx *c, const QueueItem *items, int nitems, const QReq &q, int precision, double *out_dd);
+// as run_queue, with FP32's x = 0 transforms split off into an FP64 launch
+int run_queue_sre(hm_ctx *c, const QueueItem *items, int nitems, const QReq &q, int precision, double *out_dd);
 
 // exact SRE raw sums over Gray indices [kb, ke) of a device-resident double2 state.
 // out_dd (host): [p2_hi, p2_lo, m0_hi, m0_lo, ...] for each requested q.

@@ -10,6 +10,8 @@
 // captured once as a CUDA graph and replayed.
 #include <math.h>
 
+#include <vector>
+
 #include "hm_ctx.h"
 #include "sre_kernels.cuh"
 
@@ -35,6 +37,7 @@ struct McArgs {
   const uint64_t *pd;  // nbeta x nsamples
   const double *rs;
   long long *step;  // device step counter
+  unsigned *upd_done;  // blocks of k_mc_update that finished the current step
   QParams qp;
   int n, nbeta, nsamples, U;  // nbeta: chains of this run
   int chain0, nbeta_grid;     // first chain's index in the beta grid of nbeta_grid points
@@ -139,12 +142,16 @@ __global__ void __launch_bounds__(128) k_mc_p2(McArgs a) {
 }
 
 // Metropolis update of every chain (src/SRE.jl:164-186) and next proposal.  One warp per
-// chain: for n >= 12 its lanes fold the chain's per-tile partials (lane l takes tiles l,
-// l + 32, ... in double-double, then a fixed butterfly; the order never changes), and
-// lane 0 updates the chain.
-__global__ void k_mc_update(McArgs a, int folded) {
+// chain, MC_UPD_WARPS chains per block, as many blocks as the chains need: for n >= 12
+// the warp's lanes fold the chain's per-tile partials (lane l takes tiles l, l + 32, ...
+// in double-double, then a fixed butterfly; the order never changes), and lane 0 updates
+// the chain.  The last block to finish advances the device step counter (a ticket taken
+// with an atomic after a fence, so every block has read the counter before it moves;
+// nothing waits).
+constexpr int MC_UPD_WARPS = 4;
+__global__ void __launch_bounds__(MC_UPD_WARPS * 32) k_mc_update(McArgs a, int folded) {
   const long long t = *a.step;
-  const int c = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int c = blockIdx.x * MC_UPD_WARPS + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (t < a.nsamples && c < a.nbeta) {
     Chain ch = a.ch[c];
     const uint64_t prop = ch.prop;
@@ -192,12 +199,19 @@ __global__ void k_mc_update(McArgs a, int folded) {
     }
   }
   __syncthreads();
-  if (threadIdx.x == 0 && t < a.nsamples) *a.step = t + 1;
+  if (threadIdx.x == 0) {
+    __threadfence();
+    const unsigned ticket = atomicAdd(a.upd_done, 1u);
+    if (ticket == gridDim.x - 1) {
+      *a.upd_done = 0;
+      if (t < a.nsamples) *a.step = t + 1;
+    }
+  }
 }
 
 // initial chain state: currPROB = 1e-120, currM2 = 0, currP2 = p2_0, first proposal
 __global__ void k_mc_init(McArgs a) {
-  const int c = threadIdx.x;
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c < a.nbeta) {
     Chain ch;
     ch.cur = 0;
@@ -211,7 +225,10 @@ __global__ void k_mc_init(McArgs a) {
     ch.n = 0;
     a.ch[c] = ch;
   }
-  if (c == 0) *a.step = 0;
+  if (c == 0) {
+    *a.step = 0;
+    *a.upd_done = 0;
+  }
 }
 
 // per-chain means and the Simpson combination -> out[0] = m2, out[1 + 3c ..] = (M2, M2ADD, P2)
@@ -257,7 +274,8 @@ int mc_enqueue_step(hm_ctx *c, McArgs &a) {
     const int blocks = (a.nbeta + 3) / 4;
 #define HM_MCF(NBv)                                                                             \
   case NBv:                                                                                     \
-    cudaFuncSetAttribute(k_mc_fused<NBv, QS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+    HM_CUDA(c, cudaFuncSetAttribute(k_mc_fused<NBv, QS>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                    (int)smem));                                                \
     k_mc_fused<NBv, QS><<<blocks, 128, smem, c->stream>>>(a);                                   \
     break;
     switch (nb) {
@@ -276,7 +294,7 @@ int mc_enqueue_step(hm_ctx *c, McArgs &a) {
         return set_err(c, HM_ERR_SIZE, "MC: n = %d", n);
     }
 #undef HM_MCF
-    k_mc_update<<<1, 32 * a.nbeta, 0, c->stream>>>(a, 0);
+    k_mc_update<<<(a.nbeta + MC_UPD_WARPS - 1) / MC_UPD_WARPS, MC_UPD_WARPS * 32, 0, c->stream>>>(a, 0);
   } else {
     const int hi = n - 11;
     const size_t smem = 4 * 32 * 32 * sizeof(double2);
@@ -284,8 +302,9 @@ int mc_enqueue_step(hm_ctx *c, McArgs &a) {
     const int blocks = (int)((units + 3) / 4);
 #define HM_MCP(HIv)                                                                                     \
   case HIv:                                                                                             \
-    cudaFuncSetAttribute(k_mc_p1<HIv>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);        \
-    cudaFuncSetAttribute(k_mc_p2<HIv, QS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);    \
+    HM_CUDA(c, cudaFuncSetAttribute(k_mc_p1<HIv>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
+    HM_CUDA(c, cudaFuncSetAttribute(k_mc_p2<HIv, QS>, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
+                                    (int)smem));                                                           \
     k_mc_p1<HIv><<<blocks, 128, smem, c->stream>>>(a);                                                  \
     k_mc_p2<HIv, QS><<<blocks, 128, smem, c->stream>>>(a);                                              \
     break;
@@ -304,7 +323,7 @@ int mc_enqueue_step(hm_ctx *c, McArgs &a) {
         return set_err(c, HM_ERR_SIZE, "MC: n = %d outside [1, 21]", n);
     }
 #undef HM_MCP
-    k_mc_update<<<1, 32 * a.nbeta, 0, c->stream>>>(a, 1);
+    k_mc_update<<<(a.nbeta + MC_UPD_WARPS - 1) / MC_UPD_WARPS, MC_UPD_WARPS * 32, 0, c->stream>>>(a, 1);
   }
   return HM_OK;
 }
@@ -345,11 +364,12 @@ int run_mc(hm_ctx *c, const double2 *psi, int n, double q, int nbeta_grid, int c
   HM_TRY(ensure_dev(c, (void **)&c->d_out, &c->out_cap, state_bytes));
   char *base = (char *)c->d_out;
   a.step = (long long *)base;
+  a.upd_done = (unsigned *)(base + 64);
   a.ch = (Chain *)(base + 256);
   a.part = (double *)(base + 256 + nbeta * sizeof(Chain));
   double *d_res = (double *)(base + 256 + nbeta * sizeof(Chain) + part_bytes);
   uint64_t *d_mask = (uint64_t *)(d_res + 1 + 3 * nbeta);
-  k_mc_init<<<1, 32, 0, c->stream>>>(a);
+  k_mc_init<<<(nbeta + 127) / 128, 128, 0, c->stream>>>(a);
   HM_CUDA(c, cudaGetLastError());
   // capture a block of steps once, replay it
   const int G = 16;
@@ -398,8 +418,9 @@ int mc_chains(hm_ctx *c, const double *psi, int n, double q, int nbeta, int cb, 
               const uint64_t *prop_delta, const double *rs, double *out, uint64_t *final_mask) {
   if (!psi || !prop_delta || !rs) return set_err(c, HM_ERR_ARG, "null pointer");
   if (n < 1 || n > 21) return set_err(c, HM_ERR_SIZE, "MC: n = %d outside [1, 21]", n);
-  if (nbeta < 3 || nbeta % 2 != 1 || nbeta > 32)
-    return set_err(c, HM_ERR_ARG, "Simpson needs an odd number of beta points in [3, 31] (got %d)", nbeta);
+  if (nbeta < 3 || nbeta % 2 != 1 || nbeta > HM_MC_MAX_NBETA)
+    return set_err(c, HM_ERR_ARG, "Simpson needs an odd number of beta points in [3, %d] (got %d)", HM_MC_MAX_NBETA,
+                   nbeta);
   if (cb < 0 || ce > nbeta || cb >= ce)
     return set_err(c, HM_ERR_ARG, "chain range [%d, %d) outside the %d-point beta grid", cb, ce, nbeta);
   if (nsamples < 1) return set_err(c, HM_ERR_ARG, "nsamples must be >= 1");
@@ -435,8 +456,11 @@ extern "C" int hm_mc_sre(hm_ctx *c, const double *psi, int n, double q, int nbet
   if (!c) return HM_ERR_ARG;
   c->err.clear();
   if (!out_m2 || !M2 || !M2ADD || !P2) return hm::set_err(c, HM_ERR_ARG, "null pointer");
-  double out[1 + 3 * 32];
-  HM_TRY(hm::mc_chains(c, psi, n, q, nbeta, 0, nbeta, nsamples, prop_delta, rs, out, final_mask));
+  if (nbeta < 3 || nbeta > HM_MC_MAX_NBETA)
+    return hm::set_err(c, HM_ERR_ARG, "Simpson needs an odd number of beta points in [3, %d] (got %d)",
+                       HM_MC_MAX_NBETA, nbeta);
+  std::vector<double> out(1 + 3 * (size_t)nbeta);
+  HM_TRY(hm::mc_chains(c, psi, n, q, nbeta, 0, nbeta, nsamples, prop_delta, rs, out.data(), final_mask));
   *out_m2 = out[0];
   for (int i = 0; i < nbeta; ++i) {
     M2[i] = out[1 + 3 * i];
@@ -452,8 +476,12 @@ extern "C" int hm_mc_sre_chains(hm_ctx *c, const double *psi, int n, double q, i
   if (!c) return HM_ERR_ARG;
   c->err.clear();
   if (!M2 || !M2ADD || !P2) return hm::set_err(c, HM_ERR_ARG, "null pointer");
-  double out[1 + 3 * 32];
-  HM_TRY(hm::mc_chains(c, psi, n, q, nbeta, chain_begin, chain_end, nsamples, prop_delta, rs, out, final_mask));
+  if (chain_begin < 0 || chain_end > nbeta || chain_begin >= chain_end || nbeta > HM_MC_MAX_NBETA)
+    return hm::set_err(c, HM_ERR_ARG, "chain range [%d, %d) outside the %d-point beta grid", chain_begin, chain_end,
+                       nbeta);
+  std::vector<double> out(1 + 3 * (size_t)(chain_end - chain_begin));
+  HM_TRY(hm::mc_chains(c, psi, n, q, nbeta, chain_begin, chain_end, nsamples, prop_delta, rs, out.data(),
+                       final_mask));
   for (int i = 0; i < chain_end - chain_begin; ++i) {
     M2[i] = out[1 + 3 * i];
     M2ADD[i] = out[2 + 3 * i];

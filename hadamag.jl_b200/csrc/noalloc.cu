@@ -18,7 +18,11 @@ namespace {
 
 constexpr int NOALLOC_MAX_N = HM_NOALLOC_MAX_N;    // fused path: n - 1 <= 10 element bits
 constexpr int NOALLOC_STATE = 1 << NOALLOC_MAX_N;  // double2 state slots
-constexpr int NOALLOC_WARPS = 148 * 8 * hm::FUSED_WARPS;  // partial records (148 SMs x 8 CTAs)
+// A fixed cap on the per-warp partial records, independent of the device: the grid is
+// clamped to NOALLOC_WARPS / FUSED_WARPS blocks whatever the SM count.  (4736 warps is
+// 148 SMs x 8 CTAs on a B200; on other devices the cap only changes how many X-string
+// groups each warp loops over, never the result.)
+constexpr int NOALLOC_WARPS = 148 * 8 * hm::FUSED_WARPS;
 constexpr int NOALLOC_NSUM = 5;                    // p2 + up to four moments
 constexpr int NOALLOC_DOUBLES = 2 * NOALLOC_STATE + 2 * NOALLOC_NSUM * NOALLOC_WARPS + 2 * NOALLOC_NSUM;
 
@@ -26,20 +30,48 @@ constexpr int NOALLOC_DOUBLES = 2 * NOALLOC_STATE + 2 * NOALLOC_NSUM * NOALLOC_W
 static __device__ __align__(256) double g_noalloc_scratch[NOALLOC_DOUBLES];
 
 // In host code g_noalloc_scratch names a host-side stand-in, not device memory: its
-// device address is looked up once per device (with that device current) and cached.
+// device address is looked up with the device current and cached per device, together
+// with the context it belongs to.  A device reset (cudaDeviceReset) or a destroyed and
+// recreated primary context reloads the module at another address, so the address is
+// looked up again whenever the device's current context is not the cached one.
+typedef int (*CtxGetCurrentFn)(void **);  // cuCtxGetCurrent (CUresult, CUcontext *)
 std::mutex g_noalloc_mu;
 double *g_noalloc_ptr[64] = {nullptr};
+void *g_noalloc_ctx[64] = {nullptr};
+
+CtxGetCurrentFn ctx_get_current() {
+  static std::once_flag once;
+  static CtxGetCurrentFn fn = nullptr;
+  std::call_once(once, [] {
+    void *p = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<CtxGetCurrentFn>(p);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
 
 int noalloc_scratch(int dev, double **out) {
   if (dev < 0 || dev >= 64) return HM_ERR_CUDA;
+  CtxGetCurrentFn get = ctx_get_current();
+  if (!get) return HM_ERR_CUDA;
+  void *cur = nullptr;  // null when no context is bound to this thread yet
+  if (get(&cur) != 0) return HM_ERR_CUDA;
   std::lock_guard<std::mutex> lock(g_noalloc_mu);
-  if (!g_noalloc_ptr[dev]) {
+  if (!g_noalloc_ptr[dev] || cur == nullptr || g_noalloc_ctx[dev] != cur) {
+    // the lookup binds the device's primary context to the thread when none is bound
     void *p = nullptr;
     if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || p == nullptr) {
       cudaGetLastError();
+      g_noalloc_ptr[dev] = nullptr;
       return HM_ERR_CUDA;
     }
+    if (get(&cur) != 0 || cur == nullptr) return HM_ERR_CUDA;
     g_noalloc_ptr[dev] = static_cast<double *>(p);
+    g_noalloc_ctx[dev] = cur;
   }
   *out = g_noalloc_ptr[dev];
   return HM_OK;

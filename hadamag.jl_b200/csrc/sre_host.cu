@@ -4,6 +4,7 @@
 #include <math.h>
 
 #include <mutex>
+#include <vector>
 
 #include "sre_launch.cuh"
 
@@ -137,12 +138,46 @@ static int choose_qs(const QReq &q, QParams &qp, int *idx) {
   return QS_GEN;
 }
 
+int queue_choose_qs(const QReq &q, QParams &qp, int *idx) { return choose_qs(q, qp, idx); }
+
+// Queue sweep of several states.  In FP32 the x = 0 transform of every state (F = WHT of
+// |psi|^2, whose F(0)^4 = 1 can dominate m) runs in an FP64 launch of its own and is added
+// as a double-double term, as on the stage-kernel path.
+int run_queue_sre(hm_ctx *c, const QueueItem *items, int nitems, const QReq &q, int precision, double *out_dd) {
+  const int w = 2 * (1 + q.nq);
+  if (precision != HM_FP32) return run_queue(c, items, nitems, q, HM_FP64, out_dd);
+  std::vector<QueueItem> zero, rest(items, items + nitems);
+  std::vector<int> zidx;
+  for (int i = 0; i < nitems; ++i)
+    if (items[i].kb == 0 && items[i].ke > 0) {
+      zero.push_back(QueueItem{items[i].psi, items[i].n, 0, 1});
+      zidx.push_back(i);
+      rest[i].kb = 1;
+    }
+  std::vector<double> zout(zero.size() * w);
+  double ms0 = 0.0;
+  if (!zero.empty()) {
+    HM_TRY(run_queue(c, zero.data(), (int)zero.size(), q, HM_FP64, zout.data()));
+    ms0 = c->last_ms;
+  }
+  HM_TRY(run_queue(c, rest.data(), nitems, q, HM_FP32, out_dd));
+  c->last_ms += ms0;
+  for (size_t z = 0; z < zero.size(); ++z)
+    for (int t = 0; t < 1 + q.nq; ++t) dd_add_host(out_dd + (size_t)zidx[z] * w + 2 * t, zout[z * w + 2 * t],
+                                                  zout[z * w + 2 * t + 1]);
+  return HM_OK;
+}
+
 int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, const QReq &q, int precision,
             double *out_dd) {
   if (precision == HM_PLAIN || n > 21 || n < 1) return run_sre_plain(c, psi_dev, n, kb, ke, q, out_dd);
   if (ke <= kb) {
     for (int i = 0; i < 2 * (1 + q.nq); ++i) out_dd[i] = 0.0;
     return HM_OK;
+  }
+  if (n >= 12 && queue_cfg().engine == 0) {
+    const QueueItem it{psi_dev, n, kb, ke};
+    return run_queue_sre(c, &it, 1, q, precision, out_dd);
   }
   QParams qp;
   int idx[4];
@@ -281,11 +316,14 @@ extern "C" int hm_set_param(int param, int value) {
     case HM_PARAM_BATCH:
       if (value == 0) {
         cfg.X_set = 0;
+        hm::queue_cfg().X_set = 0;
         return HM_OK;
       }
       if (value < 1 || value > 4096 || (value & (value - 1))) return HM_ERR_ARG;
       cfg.X = value;
       cfg.X_set = 1;
+      hm::queue_cfg().X = value;
+      hm::queue_cfg().X_set = 1;
       return HM_OK;
     case HM_PARAM_UNITS:
       if (value == 0) value = def.units_target;
@@ -305,6 +343,33 @@ extern "C" int hm_set_param(int param, int value) {
     case HM_PARAM_ADJ_BATCH:
       if (value < 0 || value > 1024 || (value & (value - 1))) return HM_ERR_ARG;
       cfg.adj_x = value;
+      return HM_OK;
+    case HM_PARAM_ENGINE:
+      if (value < 0 || value > 1) return HM_ERR_ARG;
+      hm::queue_cfg().engine = value;
+      return HM_OK;
+    case HM_PARAM_QUEUE_SLOTS:
+      if (value == 0) value = hm::QueueCfg().K;
+      if (value < 2 || value > 64) return HM_ERR_ARG;
+      hm::queue_cfg().K = value;
+      return HM_OK;
+    case HM_PARAM_QUEUE_SLOT_MIB:
+      if (value == 0) value = hm::QueueCfg().slot_mib;
+      if (value < 1 || value > 4096) return HM_ERR_ARG;
+      hm::queue_cfg().slot_mib = value;
+      return HM_OK;
+    case HM_PARAM_QUEUE_CHUNK:
+      if (value == 0) value = hm::QueueCfg().chunk;
+      if (value < 1 || value > 64) return HM_ERR_ARG;
+      hm::queue_cfg().chunk = value;
+      return HM_OK;
+    case HM_PARAM_QUEUE_CTAS:
+      if (value < 0 || value > 32) return HM_ERR_ARG;
+      hm::queue_cfg().ctas_per_sm = value;
+      return HM_OK;
+    case HM_PARAM_QUEUE_STALL_TEST:
+      if (value < 0 || value > 1) return HM_ERR_ARG;
+      hm::queue_cfg().stall_test = value;
       return HM_OK;
     default:
       return HM_ERR_ARG;

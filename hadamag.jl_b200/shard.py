@@ -56,6 +56,17 @@ def dd_fold(parts):
     return acc
 
 
+def dd_fold_rows(gathered):
+    """Fold the per-rank rows [p2_hi, p2_lo, m_hi, m_lo, ...] in rank order; returns one
+    row of the same layout."""
+    g = np.asarray(gathered, dtype=np.float64)
+    g = g.reshape(-1, g.shape[-1])
+    out = np.zeros(g.shape[1])
+    for j in range(0, g.shape[1], 2):
+        out[j:j + 2] = dd_fold(g[:, j:j + 2])
+    return out
+
+
 def combine_partials(gathered, n, nq):
     """gathered: array (world, 2 + 2 nq) of [p2_hi, p2_lo, m_hi, m_lo, ...] per rank.
 

@@ -38,7 +38,7 @@ extern "C" {
 #define HM_ERR_Q -3       /* unsupported Renyi index q                                */
 #define HM_ERR_CUDA -4    /* a CUDA runtime call failed (message in hm_last_error)    */
 #define HM_ERR_OOM -5     /* device allocation failed                                 */
-#define HM_ERR_TIMEOUT -6 /* reserved: no current entry point waits on the device     */
+#define HM_ERR_TIMEOUT -6 /* a bounded wait of the queue sweep gave up; no valid result */
 #define HM_ERR_ALIGN -7   /* device pointer not 16-byte aligned                      */
 
 /* precision / algorithm selector for the exact-SRE entry points */
@@ -78,6 +78,23 @@ int hm_set_stream(hm_ctx *ctx, void *cuda_stream);
 #define HM_PARAM_UNITS 3
 #define HM_PARAM_GRAPH 4
 #define HM_PARAM_ADJ_BATCH 5
+/* Knobs of the persistent queue sweep, which runs hm_sre_batched and the two-pass sizes
+ * (12 <= n <= 21) of the single-state entry points: HM_PARAM_ENGINE 0 = queue sweep
+ * (default), 1 = the stage-kernel sweep; HM_PARAM_QUEUE_SLOTS: ring slots (2..64,
+ * default 4); HM_PARAM_QUEUE_SLOT_MIB: size of a ring slot when no batch size is set or
+ * tuned (1..4096 MiB, default 16); HM_PARAM_QUEUE_CHUNK: work units a warp claims at a
+ * time (1..64, default 1); HM_PARAM_QUEUE_CTAS: CTAs per SM (1..32, 0 = as many as fit).
+ * HM_PARAM_BATCH sets the queue's X-strings per batch of the largest state as well. */
+#define HM_PARAM_ENGINE 6
+#define HM_PARAM_QUEUE_SLOTS 7
+#define HM_PARAM_QUEUE_SLOT_MIB 8
+#define HM_PARAM_QUEUE_CHUNK 9
+#define HM_PARAM_QUEUE_CTAS 10
+/* Test of the queue sweep's bounded waits: with value 1 the pass-2 units of the first
+ * batch wait for one pass-1 unit more than exist, each wait gives up after a few
+ * thousand polls, and the call returns HM_ERR_TIMEOUT with the context still usable.
+ * Value 0 (default) restores normal operation. */
+#define HM_PARAM_QUEUE_STALL_TEST 11
 int hm_set_param(int param, int value);
 
 /* Autotuner of the two-pass sweep (no reference counterpart): times the sweep of an n-qubit
@@ -158,9 +175,11 @@ int hm_sre_grad(hm_ctx *ctx, const double *psi, int n, double q, double *out_sre
  *   cuda_stream: the stream to run on (NULL = the legacy default stream); the call
  *   returns after synchronising it.  Runs on the calling thread's current device.
  * The first call on a device looks up the scratch array's device address; make that
- * first call before any stream capture.  Every call on a device shares the one array and
- * it keeps the last call's contents, so calls that overlap on the GPU (other threads,
- * other streams) race: serialise them. */
+ * first call before any stream capture.  The address is looked up again after the
+ * device's context changes (cudaDeviceReset, a recreated primary context); the first call
+ * after such a change is again a set-up call.  Every call on a device shares the one
+ * array and it keeps the last call's contents, so calls that overlap on the GPU (other
+ * threads, other streams) race: serialise them. */
 #define HM_NOALLOC_MAX_N 11
 int hm_sre_noalloc(const double *psi, int n, const double *qs, int nq, double *out_sre, double *out_lost,
                    void *cuda_stream);
@@ -175,7 +194,10 @@ int hm_sre_noalloc(const double *psi, int n, const double *qs, int nq, double *o
  * reference draws for step t of chain i (src/SRE.jl:164-170), rs[i*nsamples + t] its
  * uniform acceptance draw (src/SRE.jl:145).  Outputs: out_m2 = -log2(2^-I + I_add)
  * (Simpson), per-chain means M2[i], M2ADD[i] = m0/2^n, P2[i]; final_mask[i] (optional,
- * may be NULL) the chain's current X-string after the last step.  nbeta odd >= 3. */
+ * may be NULL) the chain's current X-string after the last step.  nbeta odd, 3 <= nbeta
+ * <= HM_MC_MAX_NBETA (the reference takes any odd count; nbeta = 1 divides by zero in its
+ * beta grid).  1 <= n <= 21. */
+#define HM_MC_MAX_NBETA 4095
 int hm_mc_sre(hm_ctx *ctx, const double *psi, int n, double q, int nbeta, int nsamples, const uint64_t *prop_delta,
               const double *rs, double *out_m2, double *M2, double *M2ADD, double *P2, uint64_t *final_mask);
 

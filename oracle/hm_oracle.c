@@ -28,6 +28,7 @@
 #include <stdlib.h>
 #include <string.h>
 #include <omp.h>
+#include <immintrin.h>
 
 #define OR_OK 0
 #define OR_ERR_ARG -1
@@ -115,66 +116,167 @@ int or_gray_general(int n, int q, int64_t *xtab, int64_t *flips) {
 /* Walsh-Hadamard transform (from the definition; see header)                 */
 /* ------------------------------------------------------------------------- */
 
-static void fwht_block(double *restrict p, int B) {
-    const int64_t bs = (int64_t)1 << B;
-    /* stages 0..2 as radix-8 on consecutive elements */
-    int s0 = 0;
-    if (B >= 3) {
-        for (int64_t i = 0; i < bs; i += 8) {
-            double a0 = p[i], a1 = p[i + 1], a2 = p[i + 2], a3 = p[i + 3];
-            double a4 = p[i + 4], a5 = p[i + 5], a6 = p[i + 6], a7 = p[i + 7];
-            double b0 = a0 + a1, b1 = a0 - a1, b2 = a2 + a3, b3 = a2 - a3;
-            double b4 = a4 + a5, b5 = a4 - a5, b6 = a6 + a7, b7 = a6 - a7;
-            double c0 = b0 + b2, c2 = b0 - b2, c1 = b1 + b3, c3 = b1 - b3;
-            double c4 = b4 + b6, c6 = b4 - b6, c5 = b5 + b7, c7 = b5 - b7;
-            p[i] = c0 + c4; p[i + 4] = c0 - c4;
-            p[i + 1] = c1 + c5; p[i + 5] = c1 - c5;
-            p[i + 2] = c2 + c6; p[i + 6] = c2 - c6;
-            p[i + 3] = c3 + c7; p[i + 7] = c3 - c7;
-        }
-        s0 = 3;
-    }
-    for (int s = s0; s < B; s++) {
-        const int64_t h = (int64_t)1 << s;
-        for (int64_t i = 0; i < bs; i += 2 * h)
+/* AVX2 implementation (the Makefile compiles for x86-64-v3).  A vector holds 4
+ * consecutive doubles: element stages 0 and 1 run inside the vector (a permute and a
+ * signed fused multiply-add each), higher stages run across vectors, three at a time on
+ * 8 vectors held in registers (radix 8). */
+
+/* radix-8 butterflies on x[0..8): pairs at distances 1, 2, 4 */
+static inline void r8(__m256d *x) {
+    for (int d = 1; d < 8; d <<= 1)
+        for (int i = 0; i < 8; i++)
+            if (!(i & d)) {
+                __m256d a = x[i], b = x[i + d];
+                x[i] = _mm256_add_pd(a, b);
+                x[i + d] = _mm256_sub_pd(a, b);
+            }
+}
+
+/* radix-4 butterflies on x[0..4): pairs at distances 1, 2 */
+static inline void r4(__m256d *x) {
+    for (int d = 1; d < 4; d <<= 1)
+        for (int i = 0; i < 4; i++)
+            if (!(i & d)) {
+                __m256d a = x[i], b = x[i + d];
+                x[i] = _mm256_add_pd(a, b);
+                x[i + d] = _mm256_sub_pd(a, b);
+            }
+}
+
+/* element stages 0 and 1 inside one vector: (a0+a1, a0-a1, ...) then pairs at distance 2 */
+static inline __m256d inv01(__m256d v) {
+    const __m256d s0 = _mm256_setr_pd(1.0, -1.0, 1.0, -1.0), s1 = _mm256_setr_pd(1.0, 1.0, -1.0, -1.0);
+    v = _mm256_fmadd_pd(v, s0, _mm256_permute_pd(v, 0x5));
+    return _mm256_fmadd_pd(v, s1, _mm256_permute4x64_pd(v, 0x4e));
+}
+
+/* element stages [s0, B) of a contiguous block of 2^B doubles (s0 >= 2) */
+static void block_stages(double *p, int B, int s0) {
+    const int64_t nv = (int64_t)1 << (B - 2);
+    int s = s0;
+    for (; s + 3 <= B; s += 3) {
+        const int64_t h = (int64_t)1 << (s - 2);
+        for (int64_t i = 0; i < nv; i += 8 * h)
             for (int64_t j = i; j < i + h; j++) {
-                double a = p[j], b = p[j + h];
-                p[j] = a + b;
-                p[j + h] = a - b;
+                __m256d x[8];
+                for (int k = 0; k < 8; k++) x[k] = _mm256_load_pd(p + 4 * (j + k * h));
+                r8(x);
+                for (int k = 0; k < 8; k++) _mm256_store_pd(p + 4 * (j + k * h), x[k]);
+            }
+    }
+    for (; s < B; s++) {
+        const int64_t h = (int64_t)1 << (s - 2);
+        for (int64_t i = 0; i < nv; i += 2 * h)
+            for (int64_t j = i; j < i + h; j++) {
+                __m256d a = _mm256_load_pd(p + 4 * j), b = _mm256_load_pd(p + 4 * (j + h));
+                _mm256_store_pd(p + 4 * j, _mm256_add_pd(a, b));
+                _mm256_store_pd(p + 4 * (j + h), _mm256_sub_pd(a, b));
             }
     }
 }
 
-/* in-place unnormalised WHT of v[0 .. 2^L) */
-void or_fwht(double *restrict v, int L) {
-    if (L <= 0) return;
+/* full transform of a contiguous, 32-byte aligned block of 2^B doubles, 2 <= B */
+static void fwht_block(double *p, int B) {
+    const int64_t nv = (int64_t)1 << (B - 2);
+    if (B >= 5) {
+        for (int64_t i = 0; i < nv; i += 8) {
+            __m256d x[8];
+            for (int k = 0; k < 8; k++) x[k] = inv01(_mm256_load_pd(p + 4 * (i + k)));
+            r8(x);
+            for (int k = 0; k < 8; k++) _mm256_store_pd(p + 4 * (i + k), x[k]);
+        }
+        block_stages(p, B, 5);
+    } else {
+        for (int64_t i = 0; i < nv; i++) _mm256_store_pd(p + 4 * i, inv01(_mm256_load_pd(p + 4 * i)));
+        block_stages(p, B, 2);
+    }
+}
+
+/* row stages [0, H) of the 2^H x bs row-major matrix v, restricted to the W columns
+ * [c, c + W) (W a multiple of 4): the high index bits of the vector */
+static void col_stages(double *v, int64_t bs, int H, int64_t c, int W) {
+    const int64_t rows = (int64_t)1 << H;
+    int s = 0;
+    for (; s + 3 <= H; s += 3) {
+        const int64_t h = (int64_t)1 << s;
+        for (int64_t i = 0; i < rows; i += 8 * h)
+            for (int64_t j = i; j < i + h; j++)
+                for (int w = 0; w < W; w += 4) {
+                    __m256d x[8];
+                    double *b = v + j * bs + c + w;
+                    for (int k = 0; k < 8; k++) x[k] = _mm256_load_pd(b + k * h * bs);
+                    r8(x);
+                    for (int k = 0; k < 8; k++) _mm256_store_pd(b + k * h * bs, x[k]);
+                }
+    }
+    if (s + 2 <= H) {
+        const int64_t h = (int64_t)1 << s;
+        for (int64_t i = 0; i < rows; i += 4 * h)
+            for (int64_t j = i; j < i + h; j++)
+                for (int w = 0; w < W; w += 4) {
+                    __m256d x[4];
+                    double *b = v + j * bs + c + w;
+                    for (int k = 0; k < 4; k++) x[k] = _mm256_load_pd(b + k * h * bs);
+                    r4(x);
+                    for (int k = 0; k < 4; k++) _mm256_store_pd(b + k * h * bs, x[k]);
+                }
+        s += 2;
+    }
+    for (; s < H; s++) {
+        const int64_t h = (int64_t)1 << s;
+        for (int64_t i = 0; i < rows; i += 2 * h)
+            for (int64_t j = i; j < i + h; j++)
+                for (int w = 0; w < W; w += 4) {
+                    double *b = v + j * bs + c + w;
+                    __m256d a = _mm256_load_pd(b), d = _mm256_load_pd(b + h * bs);
+                    _mm256_store_pd(b, _mm256_add_pd(a, d));
+                    _mm256_store_pd(b + h * bs, _mm256_sub_pd(a, d));
+                }
+    }
+}
+
+/* Split of an L-bit transform: the low B bits on contiguous blocks of 2^B doubles (16 KiB,
+ * L1-resident), then the high L-B bits on column blocks of W doubles x 2^(L-B) rows
+ * (L2-resident): two sweeps over the vector in all. */
+#define OR_FWHT_LOW_BITS 11
+#define OR_FWHT_COLS 128
+
+/* 64-byte aligned buffer of `count` doubles (at least 8) */
+static double *or_valloc(int64_t count) {
+    size_t bytes = sizeof(double) * (size_t)(count < 8 ? 8 : count);
+    bytes = (bytes + 63) & ~(size_t)63;
+    return aligned_alloc(64, bytes);
+}
+
+static void fwht_small(double *v, int L) { /* L < 2: plain butterflies */
+    if (L == 1) {
+        double a = v[0], b = v[1];
+        v[0] = a + b;
+        v[1] = a - b;
+    }
+}
+
+/* in-place unnormalised WHT of v[0 .. 2^L); v 32-byte aligned when L >= 2 */
+void or_fwht(double *v, int L) {
+    if (L <= 1) {
+        fwht_small(v, L);
+        return;
+    }
+    if (((uintptr_t)v & 31) != 0) { /* unaligned caller buffer: transform an aligned copy */
+        const size_t bytes = sizeof(double) * ((size_t)1 << L);
+        double *a = or_valloc((int64_t)1 << L);
+        memcpy(a, v, bytes);
+        or_fwht(a, L);
+        memcpy(v, a, bytes);
+        free(a);
+        return;
+    }
     const int64_t N = (int64_t)1 << L;
-    const int B = L < 11 ? L : 11; /* 16 KiB blocks stay in L1 */
+    const int B = L < OR_FWHT_LOW_BITS ? L : OR_FWHT_LOW_BITS;
     const int64_t bs = (int64_t)1 << B;
     for (int64_t base = 0; base < N; base += bs) fwht_block(v + base, B);
-    int s = B;
-    /* remaining stages two at a time (radix-4) */
-    for (; s + 1 < L; s += 2) {
-        const int64_t h = (int64_t)1 << s;
-        for (int64_t i = 0; i < N; i += 4 * h)
-            for (int64_t j = i; j < i + h; j++) {
-                double a = v[j], b = v[j + h], c = v[j + 2 * h], d = v[j + 3 * h];
-                double ab = a + b, amb = a - b, cd = c + d, cmd = c - d;
-                v[j] = ab + cd;
-                v[j + 2 * h] = ab - cd;
-                v[j + h] = amb + cmd;
-                v[j + 3 * h] = amb - cmd;
-            }
-    }
-    for (; s < L; s++) {
-        const int64_t h = (int64_t)1 << s;
-        for (int64_t i = 0; i < N; i += 2 * h)
-            for (int64_t j = i; j < i + h; j++) {
-                double a = v[j], b = v[j + h];
-                v[j] = a + b;
-                v[j + h] = a - b;
-            }
-    }
+    if (L > B)
+        for (int64_t c = 0; c < bs; c += OR_FWHT_COLS) col_stages(v, bs, L - B, c, OR_FWHT_COLS);
 }
 
 /* ------------------------------------------------------------------------- */
@@ -316,7 +418,7 @@ int or_sre_sums(const double *psi, int n, double q, int64_t istart, int64_t iend
     {
         int tid = omp_get_thread_num();
         if (tid < nthreads && tcnt[tid] > 0) {
-            double *inVR = malloc(sizeof(double) * (size_t)dim);
+            double *inVR = or_valloc(dim);
             int64_t a = istart + tdisp[tid], b = istart + tdisp[tid] + tcnt[tid] - 1;
             sre_chunk(&s, q, a, b, inVR, &acc[2 * tid], &acc[2 * tid + 1]);
             free(inVR);
@@ -329,6 +431,165 @@ int or_sre_sums(const double *psi, int n, double q, int64_t istart, int64_t iend
     }
     *p2_out = p2;
     *m_out = m;
+    free(tcnt);
+    free(tdisp);
+    free(acc);
+    sre_prep_free(&s);
+    return OR_OK;
+}
+
+/* double-double accumulation (Knuth TwoSum) for the fast path's cross-X-string sums */
+static inline void dd_acc(double *hi, double *lo, double b) {
+    double s = *hi + b, bb = s - *hi;
+    *lo += (*hi - (s - bb)) + (b - bb);
+    *hi = s;
+}
+
+/* sums of y = v^2 and y^2 (and y^3 when q3) over count doubles of p, 4-lane FP64 */
+static void moments23(const double *p, int64_t count, int q3, double *t2, double *t4, double *t6) {
+    __m256d a2 = _mm256_setzero_pd(), a4 = a2, a6 = a2, b2 = a2, b4 = a2, b6 = a2;
+    int64_t e = 0;
+    for (; e + 8 <= count; e += 8) {
+        __m256d v = _mm256_loadu_pd(p + e), w = _mm256_loadu_pd(p + e + 4);
+        __m256d y = _mm256_mul_pd(v, v), z = _mm256_mul_pd(w, w);
+        a2 = _mm256_add_pd(a2, y);
+        b2 = _mm256_add_pd(b2, z);
+        a4 = _mm256_fmadd_pd(y, y, a4);
+        b4 = _mm256_fmadd_pd(z, z, b4);
+        if (q3) {
+            a6 = _mm256_fmadd_pd(_mm256_mul_pd(y, y), y, a6);
+            b6 = _mm256_fmadd_pd(_mm256_mul_pd(z, z), z, b6);
+        }
+    }
+    double l2[4], l4[4], l6[4];
+    _mm256_storeu_pd(l2, _mm256_add_pd(a2, b2));
+    _mm256_storeu_pd(l4, _mm256_add_pd(a4, b4));
+    _mm256_storeu_pd(l6, _mm256_add_pd(a6, b6));
+    double s2 = (l2[0] + l2[1]) + (l2[2] + l2[3]), s4 = (l4[0] + l4[1]) + (l4[2] + l4[3]);
+    double s6 = (l6[0] + l6[1]) + (l6[2] + l6[3]);
+    for (; e < count; e++) {
+        const double y = p[e] * p[e];
+        s2 += y;
+        s4 += y * y;
+        s6 += y * y * y;
+    }
+    *t2 = s2;
+    *t4 = s4;
+    *t6 = s6;
+}
+
+/* v[r] = muladd(X1[r], TMP1[r^x], X2[r] TMP2[r^x]) for r in [base, base + bs), bs >= 4:
+ * vector loads at (r ^ x) with the low two bits of x applied as a lane permutation */
+static inline __m256d perm_lanes(__m256d a, int m) {
+    switch (m) {
+        case 1: return _mm256_permute_pd(a, 0x5);
+        case 2: return _mm256_permute4x64_pd(a, 0x4e);
+        case 3: return _mm256_permute4x64_pd(a, 0x1b);
+        default: return a;
+    }
+}
+static void build_block(const sre_prep *s, uint64_t x, int64_t base, int64_t bs, double *v) {
+    const int m = (int)(x & 3);
+    const uint64_t xv = x & ~(uint64_t)3;
+    for (int64_t r = base; r < base + bs; r += 4) {
+        const uint64_t j = (uint64_t)r ^ xv;
+        const __m256d t1 = perm_lanes(_mm256_loadu_pd(s->TMP1 + j), m);
+        const __m256d t2 = perm_lanes(_mm256_loadu_pd(s->TMP2 + j), m);
+        const __m256d x1 = _mm256_loadu_pd(s->X1 + r), x2 = _mm256_loadu_pd(s->X2 + r);
+        _mm256_storeu_pd(v + r, _mm256_fmadd_pd(x1, t1, _mm256_mul_pd(x2, t2)));
+    }
+}
+
+/* One thread's share of the fast path: 1-based Gray indices [ia, ib], double-double
+ * sums into a[2 (1 + nq)] (added to what a holds). */
+static void sre_fast_span(const sre_prep *s, const double *qs, int nq, int64_t ia, int64_t ib, double *a) {
+    const int n = s->n;
+    const int64_t dim = s->dim;
+    int only23 = 1, has3 = 0;
+    for (int qi = 0; qi < nq; qi++) {
+        if (qs[qi] != 2.0 && qs[qi] != 3.0) only23 = 0;
+        if (qs[qi] == 3.0) has3 = 1;
+    }
+    const int B = n < OR_FWHT_LOW_BITS ? n : OR_FWHT_LOW_BITS, H = n - B;
+    const int64_t bs = (int64_t)1 << B, rows = (int64_t)1 << H;
+    const int W = bs < OR_FWHT_COLS ? (int)bs : OR_FWHT_COLS;
+    double *v = or_valloc(dim);
+    double *col = or_valloc(rows * W);
+    for (int64_t ix = ia; ix <= ib; ix++) {
+        const uint64_t k = (uint64_t)(ix - 1), x = k ^ (k >> 1);
+        for (int64_t base = 0; base < dim; base += bs) {
+            build_block(s, x, base, bs, v);
+            fwht_block(v + base, B);
+        }
+        double xs[5][2] = {{0}};
+        for (int64_t c = 0; c < bs; c += W) {
+            if (H > 0) col_stages(v, bs, H, c, W);
+            /* gather the column block contiguously for the moment sums */
+            for (int64_t r = 0; r < rows; r++) memcpy(col + r * W, v + r * bs + c, sizeof(double) * W);
+            double t[5] = {0};
+            if (only23) {
+                double t2, t4, t6;
+                moments23(col, rows * W, has3, &t2, &t4, &t6);
+                t[0] = t2;
+                for (int qi = 0; qi < nq; qi++) t[1 + qi] = qs[qi] == 2.0 ? t4 : t6;
+            } else {
+                for (int64_t e = 0; e < rows * W; e++) {
+                    const double y = col[e] * col[e];
+                    t[0] += y;
+                    for (int qi = 0; qi < nq; qi++) t[1 + qi] += pow_q(y, qs[qi]);
+                }
+            }
+            for (int u = 0; u <= nq; u++) dd_acc(&xs[u][0], &xs[u][1], t[u]);
+        }
+        for (int u = 0; u <= nq; u++) {
+            dd_acc(&a[2 * u], &a[2 * u + 1], xs[u][0]);
+            a[2 * u + 1] += xs[u][1];
+        }
+    }
+    free(col);
+    free(v);
+}
+
+/* Fast path of or_sre_sums, several q per transform: the same Gray walk split, build
+ * (src/SRE.jl:509-540, inVR[r] = muladd(X1[r], TMP1[r^x], X2[r] TMP2[r^x]) computed
+ * straight from x, as flip_and_update_mask recomputes every entry anyway), FWHT and
+ * moments, with the build fused into the transform's low-bit sweep and the moments into
+ * its high-bit sweep, so the vector crosses memory twice per X-string.  The per-x
+ * moments are summed per column block (plain FP64 in 8 lanes) and the block sums in
+ * double-double, as are the sums across X-strings and threads; the reference's
+ * @fastmath Kahan loop (src/SRE.jl:225-278) defines no finer order.  Used for the large
+ * fixtures and the timed CPU baseline; parity tests at small n use or_sre_sums.
+ * Thread t takes the t-th contiguous partition_counts slice of [istart, iend]
+ * (src/Backends/Threads.jl:37-102); with per_thread > 0 it takes only the first
+ * per_thread indices of its slice, which is how a :threads run starts (the timed
+ * sample of the CPU baseline).
+ * out: 2 (1 + nq) doubles, (hi, lo) of sum F^2 then of sum (F^2)^q per q. */
+int or_sre_sums_fast(const double *psi, int n, const double *qs, int nq, int64_t istart, int64_t iend,
+                     int64_t per_thread, int nthreads, double *out) {
+    if (n < 2 || n > 30 || nthreads < 1 || nq < 1 || nq > 4) return OR_ERR_ARG;
+    const int64_t dim = (int64_t)1 << n;
+    if (istart < 1 || iend > dim || iend < istart - 1) return OR_ERR_ARG;
+    sre_prep s;
+    if (sre_prep_init(&s, psi, n) != OR_OK) return OR_ERR_ARG;
+    const int64_t len = iend - istart + 1;
+    int64_t *tcnt = malloc(sizeof(int64_t) * nthreads), *tdisp = malloc(sizeof(int64_t) * nthreads);
+    double *acc = calloc(2 * 5 * (size_t)nthreads, sizeof(double));
+    or_partition_counts(len, nthreads, tcnt, tdisp);
+#pragma omp parallel num_threads(nthreads)
+    {
+        int tid = omp_get_thread_num();
+        if (tid < nthreads && tcnt[tid] > 0) {
+            int64_t cnt = tcnt[tid];
+            if (per_thread > 0 && per_thread < cnt) cnt = per_thread;
+            sre_fast_span(&s, qs, nq, istart + tdisp[tid], istart + tdisp[tid] + cnt - 1, acc + 10 * (size_t)tid);
+        }
+    }
+    for (int u = 0; u < 2 * (1 + nq); u++) out[u] = 0.0;
+    for (int t = 0; t < nthreads; t++)
+        for (int u = 0; u <= nq; u++) {
+            dd_acc(&out[2 * u], &out[2 * u + 1], acc[10 * t + 2 * u]);
+            out[2 * u + 1] += acc[10 * t + 2 * u + 1];
+        }
     free(tcnt);
     free(tdisp);
     free(acc);
@@ -809,8 +1070,8 @@ int or_sre_grad(const double *psi, int n, double q, int nthreads, double *sre_ou
 #pragma omp parallel num_threads(nthreads)
     {
         int tid = omp_get_thread_num();
-        double *v = malloc(sizeof(double) * (size_t)dim);
-        double *G = malloc(sizeof(double) * (size_t)dim);
+        double *v = or_valloc(dim);
+        double *G = or_valloc(dim);
         double *g = gacc + (size_t)tid * 2 * (size_t)dim;
         double mloc = 0.0;
 #pragma omp for schedule(static)

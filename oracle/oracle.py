@@ -45,6 +45,7 @@ def lib():
         L.or_fwht.argtypes = [_dp, i]
         L.or_fht_qutrit.argtypes = [_dp, ctypes.c_int64]
         L.or_sre_sums.argtypes = [_dp, i, d, ctypes.c_int64, ctypes.c_int64, i, _dp, _dp]
+        L.or_sre_sums_fast.argtypes = [_dp, i, _dp, i, ctypes.c_int64, ctypes.c_int64, ctypes.c_int64, i, _dp]
         L.or_sre.argtypes = [_dp, i, d, i, _dp, _dp]
         L.or_naive_sre.argtypes = [_dp, i, i, i, _dp]
         L.or_mc_sre_beta.argtypes = [_dp, i, d, i, d, _u64p, _dp, _dp, _u64p]
@@ -135,6 +136,19 @@ def sre_sums(psi, q, istart, iend, nthreads=None):
     _check(lib().or_sre_sums(p, n, float(q), istart, iend, nthreads or nthreads_default(), ctypes.byref(p2),
                              ctypes.byref(m)), "sre_sums")
     return p2.value, m.value
+
+
+def sre_sums_fast(psi, qs, istart, iend, nthreads=None, per_thread=0):
+    """Double-double sums over 1-based Gray indices [istart, iend], several q per
+    transform: returns (p2 (hi, lo), m (nq, 2) as (hi, lo) rows).  per_thread > 0: each
+    thread takes only the first per_thread indices of its slice (a timed sample)."""
+    a, p = _cplx(psi)
+    n = int(np.log2(a.size))
+    q = np.ascontiguousarray(qs, dtype=np.float64).reshape(-1)
+    out = np.zeros(2 * (1 + q.size))
+    _check(lib().or_sre_sums_fast(p, n, q.ctypes.data_as(_dp), q.size, istart, iend, int(per_thread),
+                                  nthreads or nthreads_default(), out.ctypes.data_as(_dp)), "sre_sums_fast")
+    return out[:2].copy(), out[2:].reshape(q.size, 2).copy()
 
 
 def sre(psi, q, nthreads=None):
