@@ -397,7 +397,7 @@ def bench_sre(args, cfg, gpu, world, rank, dist):
                      value, world, total_ms,
                      "f64" if precision == "fp64" else "f32-butterflies/f64-reduction",
                      f"exact SRE q={qtxt}, N={n}: 2^{n} X-strings x 2^{n}-point WHT = 4^{n} Pauli strings per step",
-                     {"n": n, "q": list(qs), "precision": precision, "seed": cfg["seed"],
+                     {"n": n, "q": list(qs), "precision": precision, "seed": cfg["seed"], "engine": args.engine,
                       "parallelism": f"gray-range split x{world}", "sre": [float(v) for v in sre],
                       "lost_norm": float(lost)})
     line["roofline"] = roof
@@ -642,6 +642,7 @@ def run_ours(args):
                                 timeout=__import__("datetime").timedelta(seconds=300))
     cfg = CONFIGS[args.config]
     gpu = Gpu(local)
+    gpu.hm._native.set_param(gpu.hm._native.HM_PARAM_ENGINE, 0 if args.engine == "queue" else 1)
     kind = cfg["kind"]
     if kind == "sre":
         line = bench_sre(args, cfg, gpu, world, rank, dist)
@@ -758,6 +759,9 @@ def main():
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"],
                     help="override the configuration's precision (exact-SRE and batched configurations)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--engine", default="queue", choices=["queue", "stage"],
+                    help="two-pass sweep of the single-state entry points: the persistent queue (default) or "
+                         "the stage kernels")
     ap.add_argument("--profile-case", action="store_true", help="run the short ncu workload instead")
     ap.add_argument("--n", type=int, default=20)
     ap.add_argument("--k0", type=int, default=1024)
