@@ -21,6 +21,7 @@ import warnings
 
 import numpy as np
 
+from . import _native  # noqa: F401
 from . import shard  # noqa: F401  (multi-GPU Gray-range split)
 from ._native import (HM_FP32, HM_FP64, HM_PLAIN, PRECISIONS, ArgumentError, Context, HadaMAGError,
                       default_context, load_library)
@@ -52,8 +53,8 @@ class StateVec:
     Raises ArgumentError when the length is not a power of q (src/State.jl:40-44).
     """
 
-    def __init__(self, vec, q=2):
-        v = np.array(vec, dtype=np.complex128).reshape(-1)
+    def __init__(self, vec, q=2, copy=True):
+        v = (np.array(vec, dtype=np.complex128) if copy else np.asarray(vec, dtype=np.complex128)).reshape(-1)
         n, ok = _power_q(v.size, q)
         if not ok:
             raise ArgumentError(f"length(vec)={v.size} is not a power of q={q}")
@@ -112,10 +113,13 @@ def data(s):
 # backend selection (src/Backends/Dispatch.jl:4-90)
 
 class B200:
-    """The sm_100a backend; ``device`` selects the CUDA device."""
+    """The sm_100a backend.  ``device`` selects the CUDA device; ``devices`` (a list) runs
+    the exact SRE over several GPUs in one call, each sweeping a contiguous share of the
+    Gray range (the :mpi_cuda backend's per-node split, ext/HadaMAGMPICUDAExt.jl:49-95)."""
 
-    def __init__(self, device=0):
-        self.device = device
+    def __init__(self, device=0, devices=None):
+        self.devices = list(devices) if devices else None
+        self.device = self.devices[0] if self.devices else device
 
     def context(self):
         return default_context(self.device)
@@ -172,7 +176,10 @@ def SRE(psi, q, backend="auto", progress=False, precision="fp64", device=0):
     _progress_warning(progress)
     be = _choose_backend(backend, device)
     s = _as_state(psi, 2)
-    vals, lost = be.context().sre(s.data, (float(q),), _precision(precision))
+    if be.devices and len(be.devices) > 1:
+        vals, lost = _native.sre_multi(be.devices, s.data, (float(q),), _precision(precision))
+    else:
+        vals, lost = be.context().sre(s.data, (float(q),), _precision(precision))
     return float(vals[0]), float(lost)
 
 
@@ -272,7 +279,12 @@ def generate_gray_table(n, q):
 
 def load_state(path, q=2):
     """StateVec from disk (src/State.jl:388-404): .npy (numpy), otherwise whitespace-
-    separated real/imaginary pairs.  .jld2 needs h5py, which this image does not ship."""
+    separated real/imaginary pairs.  With a CUDA device the file is read by hm_load_state
+    straight into page-locked host memory (the state's copies to the GPU then run at full
+    link speed); without one, into an ordinary numpy array with the same contents.  .jld2
+    needs h5py, which this image does not ship."""
+    if not path.endswith(".jld2") and _cuda_available():
+        return StateVec(_native.load_state_pinned(path, q=q), q=q, copy=False)
     if path.endswith(".npy"):
         return StateVec(np.load(path), q=q)
     if path.endswith(".jld2"):
@@ -291,6 +303,14 @@ def load_state(path, q=2):
         raise ArgumentError("File does not contain real/imaginary pairs")
     v = np.array(vals[0::2]) + 1j * np.array(vals[1::2])
     return StateVec(v, q=q)
+
+
+def _cuda_available():
+    try:
+        import torch
+        return torch.cuda.is_available()
+    except Exception:
+        return False
 
 
 def reduced_density_matrix(psi, NA, side="right", q=None, device=0):

@@ -34,6 +34,8 @@ EXPORTS = [
     "hm_mc_sre", "hm_mana_pure", "hm_mana_mixed", "hm_gray_table", "hm_gray_table_general", "hm_set_param",
     "hm_last_launch_count", "hm_probe_fp64_peak", "hm_sre_noalloc", "hm_autotune",
     "hm_apply_2gate", "hm_brick_wall", "hm_reduced_density_matrix", "hm_mc_sre_chains", "hm_mana_pure_range",
+    "hm_sre_multi", "hm_sre_range_multi", "hm_multi_last_error", "hm_multi_release",
+    "hm_load_state", "hm_free_state", "hm_io_last_error", "hm_gray_table_split",
 ]
 HM_PARAM_BATCH = 1
 HM_PARAM_RING = 2
@@ -106,8 +108,18 @@ def load_library(path=None):
         L.hm_apply_2gate.argtypes = [_vp, _dp, i, i, _dp, i, i]
         L.hm_brick_wall.argtypes = [_vp, _dp, i, i, i, _dp, i]
         L.hm_reduced_density_matrix.argtypes = [_vp, _dp, i, i, i, i, _dp]
+        L.hm_sre_multi.argtypes = [_ip, i, _dp, i, _dp, i, i, _dp, _dp]
+        L.hm_sre_range_multi.argtypes = [_ip, i, _dp, i, ctypes.c_uint64, ctypes.c_uint64, _dp, i, i, _dp, _dp]
+        L.hm_multi_last_error.argtypes = []
+        L.hm_multi_last_error.restype = ctypes.c_char_p
+        L.hm_multi_release.argtypes = []
+        L.hm_gray_table_split.argtypes = [_vp, i, i, i, i, _i64p, _i64p, _i64p, _i64p]
+        L.hm_load_state.argtypes = [ctypes.c_char_p, i, ctypes.POINTER(_dp), ctypes.POINTER(ctypes.c_uint64)]
+        L.hm_free_state.argtypes = [_dp]
+        L.hm_io_last_error.argtypes = []
+        L.hm_io_last_error.restype = ctypes.c_char_p
         for name in EXPORTS:
-            if name != "hm_last_error" and name != "hm_abi_version":
+            if name not in ("hm_last_error", "hm_abi_version", "hm_multi_last_error", "hm_io_last_error"):
                 getattr(L, name).restype = i
         _lib = L
         return L
@@ -313,6 +325,24 @@ class Context:
                                            flips.ctypes.data_as(_i64p)), "hm_gray_table")
         return codes, flips[: N - 1]
 
+    def gray_table_split(self, n, q, rank, P):
+        """Rank's slice of the Gray table split over P processes (hm_gray_table_split):
+        q = 2 -> (codes uint64[cnt], flips, code_off); q > 2 -> (XTAB (n, cnt), flips, code_off)."""
+        N = q ** n
+        cap = -(-N // P)
+        width = 1 if q == 2 else n
+        codes = np.zeros(max(cap * width, 1), dtype=np.int64)
+        flips = np.zeros(max(cap, 1), dtype=np.int64)
+        off, cnt = ctypes.c_int64(), ctypes.c_int64()
+        self._check(self.lib.hm_gray_table_split(self.handle, int(n), int(q), int(rank), int(P),
+                                                 codes.ctypes.data_as(_i64p), flips.ctypes.data_as(_i64p),
+                                                 ctypes.byref(off), ctypes.byref(cnt)), "hm_gray_table_split")
+        c = cnt.value
+        fl = flips[: max(c - 1, 0)]
+        if q == 2:
+            return codes[:c].view(np.uint64), fl, off.value
+        return codes[: c * n].reshape(c, n).T.copy(), fl, off.value
+
     def apply_2gate(self, psi, q, gate, s1, s2):
         """Two-site gate on sites s1, s2 (1-based); returns the new amplitudes."""
         a = np.array(psi, dtype=np.complex128, copy=True)
@@ -393,6 +423,64 @@ def _log3_exact(size):
     if t != 1:
         raise ArgumentError(f"length(vec)={size} is not a power of q=3")
     return n
+
+
+def _multi_check(rc, what):
+    if rc == HM_OK:
+        return
+    msg = load_library().hm_multi_last_error().decode(errors="replace")
+    if rc in (HM_ERR_ARG, HM_ERR_SIZE, HM_ERR_Q, HM_ERR_ALIGN):
+        raise ArgumentError(f"{what}: {msg}")
+    raise HadaMAGError(f"{what} failed with status {rc}: {msg}")
+
+
+def sre_multi(devices, psi, qs=(2.0,), precision=HM_FP64):
+    """Exact SRE over several GPUs in one call (hm_sre_multi); returns (values, lost_norm)."""
+    L = load_library()
+    a, p = _cplx(psi)
+    n = _log2_exact(a.size)
+    d = np.ascontiguousarray(devices, dtype=np.int32)
+    q = _f64(qs)
+    out = np.zeros(q.size)
+    lost = ctypes.c_double()
+    _multi_check(L.hm_sre_multi(d.ctypes.data_as(_ip), d.size, p, n, q.ctypes.data_as(_dp), q.size, int(precision),
+                                out.ctypes.data_as(_dp), ctypes.byref(lost)), "hm_sre_multi")
+    return out, lost.value
+
+
+def sre_range_multi(devices, psi, k_begin, k_end, qs=(2.0,), precision=HM_FP64):
+    """Double-double sums of the Gray range [k_begin, k_end) split over several GPUs."""
+    L = load_library()
+    a, p = _cplx(psi)
+    n = _log2_exact(a.size)
+    d = np.ascontiguousarray(devices, dtype=np.int32)
+    q = _f64(qs)
+    p2 = np.zeros(2)
+    m = np.zeros(2 * q.size)
+    _multi_check(L.hm_sre_range_multi(d.ctypes.data_as(_ip), d.size, p, n, int(k_begin), int(k_end),
+                                      q.ctypes.data_as(_dp), q.size, int(precision), p2.ctypes.data_as(_dp),
+                                      m.ctypes.data_as(_dp)), "hm_sre_range_multi")
+    return p2, m.reshape(q.size, 2)
+
+
+def load_state_pinned(path, q=2):
+    """hm_load_state: the file's amplitudes in page-locked host memory, as a complex128
+    numpy array that frees the buffer when it is garbage-collected."""
+    import weakref
+    L = load_library()
+    ptr = _dp()
+    n = ctypes.c_uint64()
+    rc = L.hm_load_state(str(path).encode(), int(q), ctypes.byref(ptr), ctypes.byref(n))
+    if rc != HM_OK:
+        msg = L.hm_io_last_error().decode(errors="replace")
+        raise (ArgumentError if rc in (HM_ERR_ARG, HM_ERR_SIZE) else HadaMAGError)(msg)
+    buf = (ctypes.c_double * (2 * n.value)).from_address(ctypes.addressof(ptr.contents))
+    weakref.finalize(buf, L.hm_free_state, ptr)
+    return np.frombuffer(buf, dtype=np.complex128)
+
+
+def multi_release():
+    load_library().hm_multi_release()
 
 
 def set_param(param, value):

@@ -54,11 +54,12 @@ int sre_finish(const double *dd, int n, int nq, double *out_sre, double *out_los
   return HM_OK;
 }
 
-__global__ void k_gray_binary(uint64_t *codes, int64_t *flips, uint64_t N) {
+// codes of the global indices off .. off + N - 1 and the 1-based flips inside that slice
+__global__ void k_gray_binary(uint64_t *codes, int64_t *flips, uint64_t N, uint64_t off = 0) {
   for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < N; k += (uint64_t)gridDim.x * blockDim.x) {
-    const uint64_t g = gray_code(k);
+    const uint64_t g = gray_code(off + k);
     codes[k] = g;
-    if (k + 1 < N) flips[k] = (int64_t)__ffsll((long long)(g ^ gray_code(k + 1)));
+    if (k + 1 < N) flips[k] = (int64_t)__ffsll((long long)(g ^ gray_code(off + k + 1)));
   }
 }
 
@@ -77,13 +78,13 @@ __device__ void q_gray(uint64_t val, int q, int n, int64_t *out) {
   }
 }
 
-__global__ void k_gray_general(int64_t *xtab, int64_t *flips, uint64_t N, int q, int n) {
+__global__ void k_gray_general(int64_t *xtab, int64_t *flips, uint64_t N, int q, int n, uint64_t off = 0) {
   for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < N; k += (uint64_t)gridDim.x * blockDim.x) {
     int64_t a[40], b[40];
-    q_gray(k, q, n, a);
+    q_gray(off + k, q, n, a);
     for (int i = 0; i < n; ++i) xtab[k * n + i] = a[i];
     if (k + 1 < N) {
-      q_gray(k + 1, q, n, b);
+      q_gray(off + k + 1, q, n, b);
       int64_t pos = 0;
       for (int i = 0; i < n; ++i)
         if (a[i] != b[i]) {
@@ -367,6 +368,42 @@ int hm_gray_table_general(hm_ctx *c, int n, int q, int64_t *xtab, int64_t *flips
     HM_CUDA(c, cudaMemcpyAsync(xtab, c->d_aux, N * n * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
   if (N > 1)
     HM_CUDA(c, cudaMemcpyAsync(flips, c->d_aux2, (N - 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+  HM_CUDA(c, cudaStreamSynchronize(c->stream));
+  return HM_OK;
+}
+
+int hm_gray_table_split(hm_ctx *c, int n, int q, int rank, int P, int64_t *codes, int64_t *flips,
+                        int64_t *code_off, int64_t *code_cnt) {
+  if (!c) return HM_ERR_ARG;
+  c->err.clear();
+  if (P < 1 || rank < 0 || rank >= P) return set_err(c, HM_ERR_ARG, "need 0 <= rank < P (got rank %d, P %d)", rank, P);
+  if (q < 2 || q > 16 || n < 0 || n > 40) return set_err(c, HM_ERR_SIZE, "need 2 <= q <= 16, 0 <= n <= 40");
+  const double Nd = pow((double)q, n);
+  if (Nd > (double)(1ull << 30)) return set_err(c, HM_ERR_SIZE, "q^n = %g exceeds 2^30", Nd);
+  if (!code_off || !code_cnt) return set_err(c, HM_ERR_ARG, "null output pointer");
+  const uint64_t N = (uint64_t)llround(Nd);
+  // partition_counts (src/Helpers.jl:18-23): the first N mod P slices one longer
+  const uint64_t base = N / (uint64_t)P, rem = N % (uint64_t)P;
+  const uint64_t cnt = base + ((uint64_t)rank < rem ? 1 : 0);
+  const uint64_t off = (uint64_t)rank * base + std::min<uint64_t>((uint64_t)rank, rem);
+  *code_off = (int64_t)off;
+  *code_cnt = (int64_t)cnt;
+  if (cnt == 0) return HM_OK;
+  const int width = q == 2 ? 1 : n;
+  if ((!codes && width > 0) || (!flips && cnt > 1)) return set_err(c, HM_ERR_ARG, "null output pointer");
+  HM_CUDA(c, cudaSetDevice(c->device));
+  HM_TRY(ensure_dev(c, &c->d_aux, &c->aux_cap, cnt * (width > 0 ? width : 1) * sizeof(int64_t)));
+  HM_TRY(ensure_dev(c, &c->d_aux2, &c->aux2_cap, cnt * sizeof(int64_t)));
+  const unsigned blocks = (unsigned)std::min<uint64_t>((cnt + 255) / 256, (uint64_t)c->num_sms * 8);
+  if (q == 2)
+    k_gray_binary<<<blocks, 256, 0, c->stream>>>((uint64_t *)c->d_aux, (int64_t *)c->d_aux2, cnt, off);
+  else
+    k_gray_general<<<blocks, 256, 0, c->stream>>>((int64_t *)c->d_aux, (int64_t *)c->d_aux2, cnt, q, n, off);
+  HM_CUDA(c, cudaGetLastError());
+  if (width > 0)
+    HM_CUDA(c, cudaMemcpyAsync(codes, c->d_aux, cnt * width * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
+  if (cnt > 1)
+    HM_CUDA(c, cudaMemcpyAsync(flips, c->d_aux2, (cnt - 1) * sizeof(int64_t), cudaMemcpyDeviceToHost, c->stream));
   HM_CUDA(c, cudaStreamSynchronize(c->stream));
   return HM_OK;
 }

@@ -59,12 +59,16 @@ inline int set_err(hm_ctx *c, int code, const char *fmt, ...) {
   return code;
 }
 
+// On failure the runtime's error state is cleared (cudaGetLastError) so that a non-sticky
+// error is reported once, by the call that hit it, and not again by the next call's checks.
 #define HM_CUDA(c, call)                                                                              \
   do {                                                                                                \
     cudaError_t e_ = (call);                                                                          \
-    if (e_ != cudaSuccess)                                                                            \
+    if (e_ != cudaSuccess) {                                                                          \
+      cudaGetLastError();                                                                             \
       return ::hm::set_err((c), HM_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
                            __FILE__, __LINE__);                                                       \
+    }                                                                                                 \
   } while (0)
 
 #define HM_TRY(expr)          \

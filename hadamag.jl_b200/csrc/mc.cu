@@ -431,13 +431,13 @@ int mc_chains(hm_ctx *c, const double *psi, int n, double q, int nbeta, int cb, 
   const size_t ns = (size_t)nch * nsamples;
   HM_TRY(ensure_dev(c, &c->d_psi, &c->psi_cap, len * sizeof(double2)));
   HM_CUDA(c, cudaMemcpyAsync(c->d_psi, psi, len * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
-  // m0 and p2_0 of x = 0 (sample_mask!(0), src/SRE.jl:147), before the proposal stream
-  // takes the scratch buffer the plain path uses for its masks
+  // m0 and p2_0 of x = 0 (sample_mask!(0), src/SRE.jl:147): one X-string of the exact
+  // sweep, before the chains take the context's scratch buffers
   QReq qq;
   qq.nq = 1;
   qq.q[0] = q;
   double z[4];
-  HM_TRY(run_sre_plain(c, (const double2 *)c->d_psi, n, 0, 1, qq, z));
+  HM_TRY(run_sre(c, (const double2 *)c->d_psi, n, 0, 1, qq, HM_FP64, z));
   const double p2_0 = (z[0] + z[1]) / (double)len, m0 = z[2] + z[3];
   HM_TRY(ensure_dev(c, &c->d_aux, &c->aux_cap, ns * (sizeof(uint64_t) + sizeof(double))));
   uint64_t *pd = (uint64_t *)c->d_aux;

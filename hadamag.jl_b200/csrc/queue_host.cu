@@ -228,13 +228,15 @@ int run_queue(hm_ctx *c, const QueueItem *items, int nitems, const QReq &q, int 
         ce = cudaGetLastError();
       }
     if (ce != cudaSuccess) break;
-    if ((ce = cudaEventRecord(c->ev0, c->stream)) != cudaSuccess) break;
+    // external event-record nodes: the events are recorded when the graph runs (a plain
+    // cudaEventRecord during capture only adds a dependency)
+    if ((ce = cudaEventRecordWithFlags(c->ev0, c->stream, cudaEventRecordExternal)) != cudaSuccess) break;
     rc = fp64 ? launch_kind<double>(c, kind, a, cps, total, &nw_launched)
               : launch_kind<float>(c, kind, a, cps, total, &nw_launched);
     if (rc != HM_OK) break;
     k_queue_fold<<<nitems, 256, 0, c->stream>>>(d_slots, nw_launched, nitems, nsum, d_out);
     if ((ce = cudaGetLastError()) != cudaSuccess) break;
-    if ((ce = cudaEventRecord(c->ev1, c->stream)) != cudaSuccess) break;
+    if ((ce = cudaEventRecordWithFlags(c->ev1, c->stream, cudaEventRecordExternal)) != cudaSuccess) break;
     if ((ce = cudaMemcpyAsync(h_out, d_out, sizeof(double) * 2 * nsum * nitems, cudaMemcpyDeviceToHost, c->stream)) !=
         cudaSuccess)
       break;

@@ -6,6 +6,7 @@ libhadamag_b200.so (C ABI declared in include/hadamag_b200.h).
 
     using HadaMAG, HadaMAGB200
     SRE(ψ, 2; backend = HadaMAGB200.B200())
+    SRE(ψ, 2; backend = HadaMAGB200.B200(devices = [0, 1, 2, 3]))   # one call, four GPUs
     MC_SRE(ψ, 2; backend = HadaMAGB200.B200(), Nβ = 13, Nsamples = 1000, seed = 123)
     Mana(ψ3; backend = HadaMAGB200.B200())
     HadaMAGB200.Mana(ρ)                       # DensityMatrix{ComplexF64,3}
@@ -25,28 +26,48 @@ given seed reproduces the chains of the CPU backends.
 """
 module HadaMAGB200
 
-using HadaMAG
+# Explicit imports only: HadaMAG exports SRE, MC_SRE and Mana, and this module defines its
+# own functions of those names (the backend entry points _apply_backend routes to), so
+# `using HadaMAG` would bind the names to HadaMAG's functions instead.
+import HadaMAG
+using HadaMAG: StateVec, DensityMatrix, data, qubits, qudits
 using Random
 using ChainRulesCore
 
 const LIB = Ref{String}(joinpath(@__DIR__, "..", "..", "..", "libhadamag_b200.so"))
-const CTX = Ref{Ptr{Cvoid}}(C_NULL)
+const CTX = Dict{Int,Ptr{Cvoid}}()
 
 const HM_FP64 = Cint(0)
 const HM_FP32 = Cint(1)
 const HM_PLAIN = Cint(2)
 
-struct B200 <: HadaMAG.AbstractBackend end
+"""
+    B200(; device = 0, devices = nothing)
 
-function context()
-    if CTX[] == C_NULL
-        h = Ref{Ptr{Cvoid}}(C_NULL)
-        rc = ccall((:hm_create, LIB[]), Cint, (Ref{Ptr{Cvoid}}, Cint), h, 0)
-        rc == 0 || error("hm_create failed with status $rc (no usable CUDA device?)")
-        CTX[] = h[]
-        atexit(() -> ccall((:hm_destroy, LIB[]), Cint, (Ptr{Cvoid},), CTX[]))
+The sm_100a backend.  `device` selects the CUDA device; `devices` (a vector of device
+indices) runs the exact SRE over several GPUs in one call, each sweeping a contiguous
+share of the Gray range from its own host thread (`hm_sre_multi`: the per-node split of
+the :mpi_cuda backend, ext/HadaMAGMPICUDAExt.jl:49-95).
+"""
+struct B200 <: HadaMAG.AbstractBackend
+    device::Int
+    devices::Vector{Int}
+end
+B200(; device::Int = 0, devices = nothing) =
+    B200(devices === nothing ? device : first(devices), devices === nothing ? Int[] : collect(Int, devices))
+
+const CURRENT = Ref{B200}(B200())
+
+function context(dev::Int = CURRENT[].device)
+    h = get(CTX, dev, C_NULL)
+    if h == C_NULL
+        r = Ref{Ptr{Cvoid}}(C_NULL)
+        rc = ccall((:hm_create, LIB[]), Cint, (Ref{Ptr{Cvoid}}, Cint), r, dev)
+        rc == 0 || error("hm_create(device = $dev) failed with status $rc (no usable CUDA device?)")
+        h = CTX[dev] = r[]
+        atexit(() -> ccall((:hm_destroy, LIB[]), Cint, (Ptr{Cvoid},), h))
     end
-    return CTX[]
+    return h
 end
 
 # HM_ERR_ARG, HM_ERR_SIZE, HM_ERR_Q and HM_ERR_ALIGN are caller errors
@@ -57,15 +78,31 @@ function check(rc, what)
     error("$what failed with status $rc: $msg")
 end
 
+function check_multi(rc, what)
+    rc == 0 && return nothing
+    msg = unsafe_string(ccall((:hm_multi_last_error, LIB[]), Cstring, ()))
+    rc in (-1, -2, -3, -7) && throw(ArgumentError("$what: $msg"))
+    error("$what failed with status $rc: $msg")
+end
+
 function SRE(ψ, q::Number; progress = false, precision = HM_FP64, kwargs...)
     progress && @warn "Progress bar not implemented for the B200 backend."
     v = collect(ComplexF64, data(ψ))
     out = zeros(Float64, 1)
     lost = Ref{Float64}(0.0)
-    rc = ccall((:hm_sre, LIB[]), Cint,
-               (Ptr{Cvoid}, Ptr{Float64}, Cint, Ptr{Float64}, Cint, Cint, Ptr{Float64}, Ref{Float64}),
-               context(), reinterpret(Float64, v), qubits(ψ), Float64[q], 1, precision, out, lost)
-    check(rc, "hm_sre")
+    devs = CURRENT[].devices
+    if length(devs) > 1
+        rc = ccall((:hm_sre_multi, LIB[]), Cint,
+                   (Ptr{Cint}, Cint, Ptr{Float64}, Cint, Ptr{Float64}, Cint, Cint, Ptr{Float64}, Ref{Float64}),
+                   Cint.(devs), length(devs), reinterpret(Float64, v), qubits(ψ), Float64[q], 1, precision, out,
+                   lost)
+        check_multi(rc, "hm_sre_multi")
+    else
+        rc = ccall((:hm_sre, LIB[]), Cint,
+                   (Ptr{Cvoid}, Ptr{Float64}, Cint, Ptr{Float64}, Cint, Cint, Ptr{Float64}, Ref{Float64}),
+                   context(), reinterpret(Float64, v), qubits(ψ), Float64[q], 1, precision, out, lost)
+        check(rc, "hm_sre")
+    end
     return (out[1], lost[])
 end
 
@@ -225,7 +262,31 @@ function reduced_density_matrix(ψ::StateVec{T,q}, NA::Int; side::Symbol = :righ
     return DensityMatrix(ρ; q = q)
 end
 
+"""
+    load_state(path; q = 2) -> StateVec
+
+As `HadaMAG.load_state` (src/State.jl:388-404) for .npy and text files, read by
+`hm_load_state` straight into page-locked host memory and copied into the StateVec's
+vector.  .jld2 files go to `HadaMAG.load_state`.
+"""
+function load_state(path::AbstractString; q::Int = 2)
+    endswith(path, ".jld2") && return HadaMAG.load_state(path; q = q)
+    p = Ref{Ptr{Float64}}(C_NULL)
+    n = Ref{UInt64}(0)
+    rc = ccall((:hm_load_state, LIB[]), Cint, (Cstring, Cint, Ref{Ptr{Float64}}, Ref{UInt64}), path, q, p, n)
+    if rc != 0
+        msg = unsafe_string(ccall((:hm_io_last_error, LIB[]), Cstring, ()))
+        throw(ArgumentError(msg))
+    end
+    v = copy(reinterpret(ComplexF64, unsafe_wrap(Array, p[], 2 * Int(n[]))))
+    ccall((:hm_free_state, LIB[]), Cint, (Ptr{Float64},), p[])
+    return StateVec(v; q = q)
+end
+
 HadaMAG._choose_backend(b::B200) = b
-HadaMAG._apply_backend(::B200, fsym, args...; kw...) = getfield(HadaMAGB200, fsym)(args...; kw...)
+function HadaMAG._apply_backend(b::B200, fsym, args...; kw...)
+    CURRENT[] = b
+    return getfield(HadaMAGB200, fsym)(args...; kw...)
+end
 
 end # module

@@ -148,6 +148,29 @@ int hm_sre_range(hm_ctx *ctx, const double *psi, int n, uint64_t k_begin, uint64
 int hm_sre_range_dev(hm_ctx *ctx, const double *psi_dev, int n, uint64_t k_begin, uint64_t k_end,
                      const double *qs, int nq, int precision, double *p2_dd, double *m_dd);
 
+/* Exact SRE on several GPUs in one call (replaces the :mpi_cuda backend's per-rank work,
+ * SRE of ext/HadaMAGMPICUDAExt.jl:30-99): the Gray range is split into ndev nearly equal
+ * contiguous ranges (split_ranges, ext/HadaMAGMPICUDAExt.jl:8-28: the first N mod ndev
+ * one longer), devices[i] sweeps range i from its own host thread with its own context,
+ * and the double-double sums are added in list order.  A device may appear more than
+ * once.  Contexts are created on first use and kept until hm_multi_release().  Calls are
+ * serialised process-wide; errors are described by hm_multi_last_error() (per thread).
+ * psi: host pointer; other arguments and results as hm_sre. */
+int hm_sre_multi(const int *devices, int ndev, const double *psi, int n, const double *qs, int nq, int precision,
+                 double *out_sre, double *out_lost);
+
+/* Range form of hm_sre_multi: the Gray indices [k_begin, k_end) of one process (an MPI
+ * rank's share) split over its GPUs; double-double sums as hm_sre_range, to be reduced
+ * across processes by the caller. */
+int hm_sre_range_multi(const int *devices, int ndev, const double *psi, int n, uint64_t k_begin, uint64_t k_end,
+                       const double *qs, int nq, int precision, double *p2_dd, double *m_dd);
+
+/* Text of the last error of a multi-GPU call on this thread ("" when none). */
+const char *hm_multi_last_error(void);
+
+/* Destroy the contexts the multi-GPU calls keep. */
+int hm_multi_release(void);
+
 /* Batched exact SRE of many states of possibly different qubit counts in one launch
  * sequence (no reference counterpart; the reference handles one state per call).
  * psis[s] points to 2^ns[s] interleaved complex doubles (host).  For each state s and
@@ -245,6 +268,36 @@ int hm_gray_table(hm_ctx *ctx, int n, uint64_t *codes, int64_t *flips);
  * xtab is n x q^n column-major (column k = integer_to_gray(k)), flips has q^n - 1
  * 1-based digit positions.  2 <= q <= 16, q^n <= 2^26. */
 int hm_gray_table_general(hm_ctx *ctx, int n, int q, int64_t *xtab, int64_t *flips);
+
+/* Rank `rank`'s slice of the Gray table split over P processes, computed on the device,
+ * as generate_binary_splitted / generate_general_splitted of src/Basis.jl:76-106 and
+ * 206-250 (the enumeration of the reference's MPI backends): the global indices
+ * code_off .. code_off + code_cnt - 1 of the partition_counts split (src/Helpers.jl:18-23).
+ * q = 2: codes[j] = i ^ (i >> 1) (as uint64 bits); q > 2: codes is n x code_cnt
+ * column-major (column j = integer_to_gray(code_off + j)).  flips: the code_cnt - 1
+ * 1-based bit / digit positions inside the slice.  The caller sizes codes and flips for
+ * the slice (at most ceil(q^n / P) columns).  q^n <= 2^30. */
+int hm_gray_table_split(hm_ctx *ctx, int n, int q, int rank, int P, int64_t *codes, int64_t *flips,
+                        int64_t *code_off, int64_t *code_cnt);
+
+/* ---------------------------------------------------------------------------------- */
+/* State files                                                                          */
+/* ---------------------------------------------------------------------------------- */
+
+/* Read a state file into page-locked host memory (replaces load_state of
+ * src/State.jl:388-404): ".npy" (a complex128 vector, or float64 read as real amplitudes)
+ * with one read straight into the buffer, any other name as whitespace-separated real /
+ * imaginary pairs.  ".jld2" (HDF5) returns HM_ERR_ARG: this library reads no HDF5.
+ * *psi_pinned receives 2 *len doubles (interleaved complex) from cudaMallocHost, to be
+ * released with hm_free_state; *len must be a power of q (HM_ERR_SIZE otherwise, as the
+ * reference's StateVec check).  Errors are described by hm_io_last_error() (per thread). */
+int hm_load_state(const char *path, int q, double **psi_pinned, uint64_t *len);
+
+/* Release a buffer from hm_load_state. */
+int hm_free_state(double *psi_pinned);
+
+/* Text of the last error of hm_load_state on this thread ("" when none). */
+const char *hm_io_last_error(void);
 
 /* ---------------------------------------------------------------------------------- */
 /* State preparation (inputs of the SRE and Mana paths)                                 */

@@ -1059,21 +1059,24 @@ int or_mana_mixed(const double *rho, int N, double *mana_out, double *w_out) {
  * s = r ^ x, g_x(r) = X1[r] T1[s] + X2[r] T2[s] (T1 = X1 + X2, T2 = X2 - X1):
  *   dm/dX1[r] += G(r) T1[s],  dm/dX2[r] += G(r) T2[s],
  *   dm/dX1[s] += G(r) (X1[r] - X2[r]),  dm/dX2[s] += G(r) (X1[r] + X2[r]).
- * dSRE = -dm / (m ln 2).  grad is interleaved (d/dRe, d/dIm). */
+ * dSRE = -dm / (m ln 2).  grad is interleaved (d/dRe, d/dIm).  The sums across X-strings
+ * (m and every gradient entry) are double-double, so the only roundings left are those of
+ * each X-string's own transform. */
 int or_sre_grad(const double *psi, int n, double q, int nthreads, double *sre_out, double *grad) {
     if (n < 1 || n > 22 || nthreads < 1) return OR_ERR_ARG;
     sre_prep s;
     if (sre_prep_init(&s, psi, n) != OR_OK) return OR_ERR_ARG;
     const int64_t dim = s.dim;
-    double *gacc = calloc((size_t)nthreads * 2 * (size_t)dim, sizeof(double));
-    double *macc = calloc((size_t)nthreads, sizeof(double));
+    /* per thread: gradient (hi, lo) pairs, 4 doubles per amplitude */
+    double *gacc = calloc((size_t)nthreads * 4 * (size_t)dim, sizeof(double));
+    double *macc = calloc(2 * (size_t)nthreads, sizeof(double));
 #pragma omp parallel num_threads(nthreads)
     {
         int tid = omp_get_thread_num();
         double *v = or_valloc(dim);
         double *G = or_valloc(dim);
-        double *g = gacc + (size_t)tid * 2 * (size_t)dim;
-        double mloc = 0.0;
+        double *g = gacc + (size_t)tid * 4 * (size_t)dim;
+        double mhi = 0.0, mlo = 0.0;
 #pragma omp for schedule(static)
         for (int64_t x = 0; x < dim; x++) {
             for (int64_t r = 0; r < dim; r++) {
@@ -1081,33 +1084,43 @@ int or_sre_grad(const double *psi, int n, double q, int nthreads, double *sre_ou
                 v[r] = fma(s.X1[r], s.TMP1[j], s.X2[r] * s.TMP2[j]);
             }
             or_fwht(v, n);
+            double mx = 0.0;
             for (int64_t k = 0; k < dim; k++) {
                 double F = v[k], p = F * F;
-                mloc += pow_q(p, q);
+                mx += pow_q(p, q);
                 /* d/dF (F^2)^q = 2 q F^(2q-1) = 2 q p^(q-1) F */
                 G[k] = 2.0 * q * (q == 2.0 ? p : pow(p, q - 1.0)) * F;
             }
+            dd_acc(&mhi, &mlo, mx);
             or_fwht(G, n);
             for (int64_t r = 0; r < dim; r++) {
                 uint64_t sidx = (uint64_t)r ^ (uint64_t)x;
                 double gr = G[r];
-                g[2 * r] += gr * s.TMP1[sidx];
-                g[2 * r + 1] += gr * s.TMP2[sidx];
-                g[2 * sidx] += gr * (s.X1[r] - s.X2[r]);
-                g[2 * sidx + 1] += gr * (s.X1[r] + s.X2[r]);
+                dd_acc(&g[4 * r], &g[4 * r + 1], gr * s.TMP1[sidx]);
+                dd_acc(&g[4 * r + 2], &g[4 * r + 3], gr * s.TMP2[sidx]);
+                dd_acc(&g[4 * sidx], &g[4 * sidx + 1], gr * (s.X1[r] - s.X2[r]));
+                dd_acc(&g[4 * sidx + 2], &g[4 * sidx + 3], gr * (s.X1[r] + s.X2[r]));
             }
         }
-        macc[tid] = mloc;
+        macc[2 * tid] = mhi;
+        macc[2 * tid + 1] = mlo;
         free(v);
         free(G);
     }
-    double m = 0.0;
-    for (int t = 0; t < nthreads; t++) m += macc[t];
+    double mh = 0.0, ml = 0.0;
+    for (int t = 0; t < nthreads; t++) {
+        dd_acc(&mh, &ml, macc[2 * t]);
+        ml += macc[2 * t + 1];
+    }
+    const double m = mh + ml;
     const double scale = -1.0 / (m * log(2.0));
     for (int64_t i = 0; i < 2 * dim; i++) {
-        double a = 0.0;
-        for (int t = 0; t < nthreads; t++) a += gacc[(size_t)t * 2 * (size_t)dim + (size_t)i];
-        grad[i] = scale * a;
+        double ah = 0.0, al = 0.0;
+        for (int t = 0; t < nthreads; t++) {
+            dd_acc(&ah, &al, gacc[(size_t)t * 4 * (size_t)dim + 2 * (size_t)i]);
+            al += gacc[(size_t)t * 4 * (size_t)dim + 2 * (size_t)i + 1];
+        }
+        grad[i] = scale * (ah + al);
     }
     *sre_out = -log2(m / (double)dim);
     free(gacc);

@@ -118,3 +118,23 @@ def test_queue_wait_that_gives_up_reports_timeout(ctx, hm, knobs):
     knobs(hm._native.HM_PARAM_ENGINE, 1)
     w, _ = ctx.sre(psi, (2.0,), hm.HM_FP64)
     assert v[0] == pytest.approx(w[0], rel=1e-13)
+
+
+def test_sre_multi_matches_single_device(hm, ctx):
+    """hm_sre_multi on one GPU listed one, two and three times: the threads, the range split
+    and the double-double combine give the single-call value."""
+    n = 16
+    psi = rand_state(1 << n, 61)
+    ref, rlost = ctx.sre(psi, (2.0, 3.0), hm.HM_FP64)
+    for devs in ([0], [0, 0], [0, 0, 0]):
+        v, lost = hm._native.sre_multi(devs, psi, (2.0, 3.0), hm.HM_FP64)
+        assert np.allclose(v, ref, rtol=1e-13)
+        assert lost == pytest.approx(rlost, abs=1e-14)
+    p2, m = hm._native.sre_range_multi([0, 0], psi, 1000, 5000, (2.0,), hm.HM_FP64)
+    r2, rm = ctx.sre_range(psi, 1000, 5000, (2.0,), hm.HM_FP64)
+    assert _dd(p2) == pytest.approx(_dd(r2), rel=1e-14) and _dd(m[0]) == pytest.approx(_dd(rm[0]), rel=1e-14)
+    v, _ = hm.SRE(hm.StateVec(psi), 2, backend=hm.B200(devices=[0, 0]))
+    assert v == pytest.approx(ref[0], rel=1e-13)
+    with pytest.raises(hm.ArgumentError):
+        hm._native.sre_multi([], psi, (2.0,), hm.HM_FP64)
+    hm._native.multi_release()

@@ -143,3 +143,26 @@ def test_autotune_records_a_batch_size(ctx, hm, oracle):
         assert v[0] == close(ref, prec)
     with pytest.raises(hm.ArgumentError):
         ctx.autotune(11, hm.HM_FP64)
+
+
+def test_split_gray_tables_match_oracle(ctx, oracle):
+    """generate_binary_splitted / generate_general_splitted (src/Basis.jl:76-106, 206-250):
+    every rank's slice bit-exact, and the slices concatenate to the whole table."""
+    for n, P in [(5, 3), (10, 4), (11, 7), (3, 16)]:
+        full, _ = ctx.gray_table(n)
+        got = []
+        for r in range(P):
+            c, f, off = ctx.gray_table_split(n, 2, r, P)
+            co, fo, oo = oracle.gray_binary_split(n, r, P)
+            assert off == oo and np.array_equal(c, co) and np.array_equal(f, fo)
+            got.append(c)
+        assert np.array_equal(np.concatenate(got), full)
+    for n, q, P in [(4, 3, 5), (6, 3, 4)]:
+        xt, _ = ctx.gray_table_general(n, q)
+        cols = []
+        for r in range(P):
+            x, f, off = ctx.gray_table_split(n, q, r, P)
+            cols.append(x)
+            if x.shape[1] > 1:
+                assert np.array_equal(f, [int(np.argmax(x[:, j] != x[:, j + 1])) + 1 for j in range(x.shape[1] - 1)])
+        assert np.array_equal(np.concatenate(cols, axis=1), xt)

@@ -113,3 +113,27 @@ def test_mana_range_argument_errors(hm, ctx):
     for a, b in ((0, 0), (5, 3), (-1, 4), (0, 82)):
         with pytest.raises(hm.ArgumentError):
             ctx.mana_pure_range(psi, a, b)
+
+
+def test_load_state_pinned_matches_numpy(hm, tmp_path):
+    """hm_load_state reads .npy and text files into page-locked memory with the same
+    amplitudes numpy reads; the buffer is registered with CUDA as host-pinned."""
+    psi = rand_state(1 << 9, 9)
+    p = tmp_path / "s.npy"
+    np.save(p, psi)
+    s = hm.load_state(str(p))
+    assert np.array_equal(s.data, psi) and s.n == 9
+    import torch
+    assert torch.from_numpy(s.data.view(np.float64)).is_pinned()
+    t = tmp_path / "s.txt"
+    t.write_text("\n".join(f"{z.real!r} {z.imag!r}" for z in psi))
+    assert np.array_equal(hm.load_state(str(t)).data, psi)
+    np.save(tmp_path / "r.npy", psi.real)
+    assert np.array_equal(hm.load_state(str(tmp_path / "r.npy")).data, psi.real.astype(complex))
+    np.save(tmp_path / "bad.npy", psi[:100])
+    with pytest.raises(hm.ArgumentError):
+        hm.load_state(str(tmp_path / "bad.npy"))
+    with pytest.raises(hm.ArgumentError):
+        hm.load_state(str(tmp_path / "s.jld2"))
+    v, _ = hm.SRE(s, 2)
+    assert v == pytest.approx(hm.SRE(hm.StateVec(psi), 2)[0], rel=1e-15)
