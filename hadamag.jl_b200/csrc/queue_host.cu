@@ -205,8 +205,12 @@ int run_queue(hm_ctx *c, const QueueItem *items, int nitems, const QReq &q, int 
       const int HI = n - 11, C = 1 << (10 - HI), NT = 1024 / C;
       a.xcap[ti] = (int)(slot_elems >> (n - 1));
       a.geom[ti] = ring_tma_geom(C, NT);
-      if (!encode_ring_tmap(&a.tmap[ti], a.ring, fp64 ? 8 : 4, C, 1 << HI, NT, K * a.xcap[ti],
-                            ((uint64_t)1 << (n - 1)) * vbytes, a.geom[ti]))
+      // a tile row narrower than 16 bytes (FP32 at n = 21) has no tensor map: plain stores
+      a.tma[ti] = encode_ring_tmap(&a.tmap[ti], a.ring, fp64 ? 8 : 4, C, 1 << HI, NT, K * a.xcap[ti],
+                                   ((uint64_t)1 << (n - 1)) * vbytes, a.geom[ti])
+                      ? 1
+                      : 0;
+      if (!a.tma[ti] && 2 * C * (fp64 ? 8 : 4) >= 16)
         return set_err(c, HM_ERR_CUDA, "queue sweep: tensor map of the n = %d ring could not be encoded", n);
     }
   }

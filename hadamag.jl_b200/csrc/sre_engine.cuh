@@ -25,6 +25,7 @@
 // (conflict-free 16-byte / 8-byte accesses).
 #pragma once
 #include "hm_common.cuh"
+#include "tmem_transpose.cuh"
 
 namespace hm {
 
@@ -62,6 +63,65 @@ __device__ __forceinline__ void transpose_ab(V (&v)[R], V *sm, int lane) {
     v[i] = sm[e ^ ((e >> LOGR) & SW)];
   }
   __syncwarp();
+}
+
+// ---------------------------------------------------------------------------------
+// Lane <-> register exchanges through tensor memory (tmem_transpose.cuh).  A two-pass unit
+// must move the five element bits held by the lane number into registers once per pass.
+// Through shared memory that is a 32 KB store + load per warp unit on the L1/shared data
+// path, which the ring gathers and stores also use; through TMEM it is three (pass 1) or
+// at most three (pass 2) store/load rounds on the tensor-memory path (measured on B200:
+// about 3x the shared-memory rate, and a separate datapath).  A CTA allocates the columns
+// once; each warp uses its own 32 lanes (warp w of the CTA reaches lanes 32 (w mod 4) ..).
+template <typename T> struct TmemCols { static constexpr int value = sizeof(T) == 8 ? 128 : 64; };
+
+__device__ __forceinline__ uint32_t tmem_cta_alloc(uint32_t *slot, int ncols) {
+  if (threadIdx.x < 32) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(slot);
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(s), "r"(ncols) : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  return *(volatile uint32_t *)slot;
+}
+
+// every warp of the CTA must have finished its TMEM accesses
+__device__ __forceinline__ void tmem_cta_free(uint32_t base, int ncols) {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (threadIdx.x < 32) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(base), "r"(ncols) : "memory");
+}
+
+// this warp's lanes of the CTA's allocation
+__device__ __forceinline__ uint32_t tmem_warp_addr(uint32_t base) {
+  return base + ((uint32_t)(32 * ((threadIdx.x >> 5) & 3)) << 16);
+}
+
+// pass-1 row: lanes e0..e4 / registers e5..e9 in, registers e0..e4 out (register i =
+// element bits of i), the lane number a fixed relabelling of e5..e9
+__device__ __forceinline__ void tmem_row(double2 (&v)[32], uint32_t ta) { tmem_xchg_row_f64(v, ta); }
+__device__ __forceinline__ void tmem_row(float2 (&v)[32], uint32_t ta) { tmem_xchg_row_f32(v, ta); }
+
+// pass-2 tile of 2^HI rows (6 <= HI <= 10): the row bits on lanes go to registers, lowest
+// row bit at register bit 0; afterwards register bits 0 .. HI - 6 hold the rows still to
+// transform
+template <int HI, typename V>
+__device__ __forceinline__ void tmem_tile(V (&v)[32], uint32_t ta) {
+  constexpr bool F64 = sizeof(V) == 16;
+  if constexpr (HI == 6) {
+    if constexpr (F64) tmem_xchg_tile6_f64(v, ta); else tmem_xchg_tile6_f32(v, ta);
+  } else if constexpr (HI == 7) {
+    if constexpr (F64) tmem_xchg_tile7_f64(v, ta); else tmem_xchg_tile7_f32(v, ta);
+  } else if constexpr (HI == 8) {
+    if constexpr (F64) tmem_xchg_tile8_f64(v, ta); else tmem_xchg_tile8_f32(v, ta);
+  } else if constexpr (HI == 9) {
+    if constexpr (F64) tmem_xchg_tile9_f64(v, ta); else tmem_xchg_tile9_f32(v, ta);
+  } else if constexpr (HI == 10) {
+    if constexpr (F64) tmem_xchg_tile10_f64(v, ta); else tmem_xchg_tile10_f32(v, ta);
+  }
 }
 
 // ---------------------------------------------------------------------------------
@@ -334,14 +394,20 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 // As p1_unit, with the row leaving through the warp's shared buffer and tensor stores.
 // The caller waits for the stores to have read the buffer (bulk_wait_read_all on lane 0,
 // then __syncwarp) before the buffer's next use.
-template <int R, int HI, typename V, typename Pre = NoHook>
+template <int R, int HI, bool TM, typename V, typename Pre = NoHook>
 __device__ __forceinline__ void p1_unit_tma(const V *__restrict__ psi, const XInfo &xi, uint64_t rho, V *sm, int lane,
-                                            const void *tmap, const TmaGeom &g, int xcoord, const Pre &pre = Pre()) {
+                                            const void *tmap, const TmaGeom &g, int xcoord, uint32_t ta,
+                                            const Pre &pre = Pre()) {
   constexpr int LOGR = ilog2c(R);
   V v[R];
   p1_build<R, false>(v, psi, xi, rho, sm, lane);
   reg_wht<R, 0, LOGR>(v);
-  transpose_ab<R>(v, sm, lane);
+  if constexpr (TM) {
+    static_assert(R == 32, "the TMEM exchanges are generated for 32 values per lane");
+    tmem_row(v, ta);
+  } else {
+    transpose_ab<R>(v, sm, lane);
+  }
   reg_wht<R, 0, 5>(v);
   // register i of lane l holds element k = R l + i, kept at position p = 32 i + l
 #pragma unroll
@@ -360,9 +426,9 @@ __device__ __forceinline__ void p1_unit_tma(const V *__restrict__ psi, const XIn
 
 // Pass 2: tile of 2^HI rows x C = 2^(PB-HI) positions of one X-string's intermediate
 // (one contiguous block); transform over the row bits, then per-lane moments.
-template <int R, int HI, int QS, typename V>
+template <int R, int HI, int QS, bool TM = false, typename V>
 __device__ __forceinline__ void p2_unit(const V *__restrict__ tile_ptr, V *sm, int lane, double *s,
-                                        const QParams &qp) {
+                                        const QParams &qp, uint32_t ta = 0) {
   constexpr int LOGR = ilog2c(R), PB = LOGR + 5, LOGC = PB - HI;
   static_assert(HI >= 1 && HI <= PB, "pass-2 bits out of range");
   V v[R];
@@ -370,6 +436,10 @@ __device__ __forceinline__ void p2_unit(const V *__restrict__ tile_ptr, V *sm, i
   for (int i = 0; i < R; ++i) v[i] = __ldcg(tile_ptr + i * 32 + lane);
   if constexpr (LOGC >= 5) {
     reg_wht<R, LOGC - 5, LOGR>(v);
+  } else if constexpr (TM && R == 32) {
+    reg_wht<R, 0, LOGR>(v);
+    tmem_tile<HI>(v, ta);
+    reg_wht<R, 0, 5 - LOGC>(v);
   } else {
     reg_wht<R, 0, LOGR>(v);
     transpose_ab<R>(v, sm, lane);

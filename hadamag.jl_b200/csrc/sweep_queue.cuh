@@ -70,6 +70,7 @@ struct QArgs {
   CUtensorMap tmap[QMAX_TMAPS];  // ring views per two-pass n (index n - 12)
   TmaGeom geom[QMAX_TMAPS];
   int xcap[QMAX_TMAPS];  // X-string positions per slot for that n (slot_elems / 2^(n-1))
+  int tma[QMAX_TMAPS];   // 1: pass 1 stores through the tensor map; 0: plain stores
   const QState *st;
   void *ring;
   unsigned *done1, *done2;  // per global batch
@@ -137,6 +138,10 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   V *sm = reinterpret_cast<V *>(smem_q) + warp * (32 * R);
   const int gwarp = blockIdx.x * QWARPS + warp;
+  // TMEM for the two-pass units' lane <-> register exchanges
+  __shared__ uint32_t tmem_slot;
+  const uint32_t tmem_base = tmem_cta_alloc(&tmem_slot, TmemCols<T>::value);
+  const uint32_t ta = tmem_warp_addr(tmem_base);
   dd acc[NQ + 1];
 #pragma unroll
   for (int t = 0; t <= NQ; ++t) acc[t] = dd{0.0, 0.0};
@@ -324,23 +329,39 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
           }
         }
         reg_wht<R, 0, 5>(v);
-        transpose_ab<R>(v, sm, lane);
+        tmem_row(v, ta);
         reg_wht<R, 0, 5>(v);
+        if (a.tma[ti]) {
 #pragma unroll
-        for (int i = 0; i < R; ++i) sm[i * 32 + lane] = v[i];
-        fence_proxy_async_smem();
-        __syncwarp();
-        announce();  // the previous unit's stores completed long ago in most cases
-        if (lane == 0) {
-          const TmaGeom g = a.geom[ti];
-          const int xcoord = slot * xcap + xs;
-          for (int b2 = 0; b2 < g.nb2; ++b2)
-            for (int b0 = 0; b0 < g.nb0; ++b0)
-              tma_store_4d(&a.tmap[ti], sm + (size_t)b2 * g.box2 * g.C + (size_t)b0 * (g.box0 / 2), b0 * g.box0,
-                           (int)sub, b2 * g.box2, xcoord);
-          bulk_commit();
+          for (int i = 0; i < R; ++i) sm[i * 32 + lane] = v[i];
+          fence_proxy_async_smem();
+          __syncwarp();
+          announce();  // the previous unit's stores completed long ago in most cases
+          if (lane == 0) {
+            const TmaGeom g = a.geom[ti];
+            const int xcoord = slot * xcap + xs;
+            for (int b2 = 0; b2 < g.nb2; ++b2)
+              for (int b0 = 0; b0 < g.nb0; ++b0)
+                tma_store_4d(&a.tmap[ti], sm + (size_t)b2 * g.box2 * g.C + (size_t)b0 * (g.box0 / 2), b0 * g.box0,
+                             (int)sub, b2 * g.box2, xcoord);
+            bulk_commit();
+          }
+          pending = q;
+        } else {
+          // tile rows too narrow for a tensor map (FP32 at n = 21: 8 bytes): plain stores of
+          // position p = 32 i + lane to tile p >> LOGC, column p mod C
+          const int LOGC = PB - hi;
+#pragma unroll
+          for (int i = 0; i < R; ++i) {
+            const uint32_t pp = (uint32_t)(i * 32 + lane);
+            const uint32_t t = pp >> LOGC, cc = pp & ((1u << LOGC) - 1u);
+            __stcg(inter_x + (((size_t)t << (hi + LOGC)) + (sub << LOGC) + cc), v[i]);
+          }
+          __threadfence();
+          __syncwarp();
+          announce();
+          if (lane == 0) atomicAdd(a.done1 + q, 1u);
         }
-        pending = q;
       } else {
         announce();
         if (lane == 0) atomicAdd(a.done1 + q, 1u);
@@ -358,8 +379,14 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
           reg_wht_rt<R>(v, LOGC - 5, 5);
         } else {
           reg_wht<R, 0, 5>(v);
-          transpose_ab<R>(v, sm, lane);
-          reg_wht_rt<R>(v, LOGC, 5);
+          switch (hi) {  // warp-uniform
+            case 6: tmem_tile<6>(v, ta); break;
+            case 7: tmem_tile<7>(v, ta); break;
+            case 8: tmem_tile<8>(v, ta); break;
+            case 9: tmem_tile<9>(v, ta); break;
+            default: tmem_tile<10>(v, ta); break;
+          }
+          reg_wht_rt<R>(v, 0, 5 - LOGC);
         }
         double sums[NQ + 1];
         lane_moments<R, QS>(v, sums, a.qp, sm, lane);
@@ -379,6 +406,7 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
   announce();
   if (dirty) flush();
   if (lane == 0) bulk_wait_all();
+  tmem_cta_free(tmem_base, TmemCols<T>::value);
 }
 
 // fold of every warp's slot of each state, in warp order: out[s][2t], out[s][2t + 1]

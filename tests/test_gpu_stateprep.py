@@ -126,7 +126,7 @@ def test_load_state_pinned_matches_numpy(hm, tmp_path):
     import torch
     assert torch.from_numpy(s.data.view(np.float64)).is_pinned()
     t = tmp_path / "s.txt"
-    t.write_text("\n".join(f"{z.real!r} {z.imag!r}" for z in psi))
+    t.write_text("\n".join(f"{float(z.real)!r} {float(z.imag)!r}" for z in psi))
     assert np.array_equal(hm.load_state(str(t)).data, psi)
     np.save(tmp_path / "r.npy", psi.real)
     assert np.array_equal(hm.load_state(str(tmp_path / "r.npy")).data, psi.real.astype(complex))
