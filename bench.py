@@ -642,7 +642,7 @@ def run_ours(args):
                                 timeout=__import__("datetime").timedelta(seconds=300))
     cfg = CONFIGS[args.config]
     gpu = Gpu(local)
-    gpu.hm._native.set_param(gpu.hm._native.HM_PARAM_ENGINE, 0 if args.engine == "queue" else 1)
+    gpu.hm._native.set_param(gpu.hm._native.HM_PARAM_ENGINE, {"auto": 0, "stage": 1, "queue": 2}[args.engine])
     kind = cfg["kind"]
     if kind == "sre":
         line = bench_sre(args, cfg, gpu, world, rank, dist)
@@ -728,6 +728,7 @@ def profile_case(args):
     of a seeded L-qutrit state (--mana L).  Prints the sums and the device time."""
     import hadamag_b200 as hm
     hm._native.set_param(hm._native.HM_PARAM_ADJ_BATCH, args.adj_batch)
+    hm._native.set_param(hm._native.HM_PARAM_ENGINE, {"auto": 0, "stage": 1, "queue": 2}[args.engine])
     ctx = hm._native.default_context(0)
     if args.mana:
         v = make_state(3 ** args.mana, args.mana)
@@ -759,9 +760,9 @@ def main():
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"],
                     help="override the configuration's precision (exact-SRE and batched configurations)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--engine", default="queue", choices=["queue", "stage"],
-                    help="two-pass sweep of the single-state entry points: the persistent queue (default) or "
-                         "the stage kernels")
+    ap.add_argument("--engine", default="auto", choices=["auto", "stage", "queue"],
+                    help="two-pass sweep of the single-state entry points: automatic (the tuned choice, else "
+                         "the stage kernels), the stage kernels or the persistent queue")
     ap.add_argument("--profile-case", action="store_true", help="run the short ncu workload instead")
     ap.add_argument("--n", type=int, default=20)
     ap.add_argument("--k0", type=int, default=1024)

@@ -35,7 +35,7 @@ EXPORTS = [
     "hm_last_launch_count", "hm_probe_fp64_peak", "hm_sre_noalloc", "hm_autotune",
     "hm_apply_2gate", "hm_brick_wall", "hm_reduced_density_matrix", "hm_mc_sre_chains", "hm_mana_pure_range",
     "hm_sre_multi", "hm_sre_range_multi", "hm_multi_last_error", "hm_multi_release",
-    "hm_load_state", "hm_free_state", "hm_io_last_error", "hm_gray_table_split",
+    "hm_load_state", "hm_free_state", "hm_io_last_error", "hm_gray_table_split", "hm_autotune_choice",
 ]
 HM_PARAM_BATCH = 1
 HM_PARAM_RING = 2
@@ -113,6 +113,7 @@ def load_library(path=None):
         L.hm_multi_last_error.argtypes = []
         L.hm_multi_last_error.restype = ctypes.c_char_p
         L.hm_multi_release.argtypes = []
+        L.hm_autotune_choice.argtypes = [i, i, _ip, _ip, _ip]
         L.hm_gray_table_split.argtypes = [_vp, i, i, i, i, _i64p, _i64p, _i64p, _i64p]
         L.hm_load_state.argtypes = [ctypes.c_char_p, i, ctypes.POINTER(_dp), ctypes.POINTER(ctypes.c_uint64)]
         L.hm_free_state.argtypes = [_dp]
@@ -481,6 +482,16 @@ def load_state_pinned(path, q=2):
 
 def multi_release():
     load_library().hm_multi_release()
+
+
+def autotune_choice(n, precision=HM_FP64):
+    """(engine, batch, CTAs per SM) that hm_autotune recorded for (n, precision); engine
+    0 = not tuned, 1 = stage kernels, 2 = queue sweep."""
+    e, b, c = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    rc = load_library().hm_autotune_choice(int(n), int(precision), ctypes.byref(e), ctypes.byref(b), ctypes.byref(c))
+    if rc != HM_OK:
+        raise ArgumentError(f"hm_autotune_choice({n}, {precision}) rejected")
+    return e.value, b.value, c.value
 
 
 def set_param(param, value):

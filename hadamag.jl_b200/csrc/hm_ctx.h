@@ -138,12 +138,14 @@ struct QueueCfg {
   int K = 4;
   int chunk = 1;
   int ctas_per_sm = 0;
-  int engine = 0;  // single-state sweeps: 0 queue, 1 stage kernels
+  int engine = 0;  // single-state sweeps: 0 automatic, 1 stage kernels, 2 queue sweep
   int stall_test = 0;  // test of the bounded waits (HM_PARAM_QUEUE_STALL_TEST)
   int tuned_x[2][32] = {};
   int tuned_cps[2][32] = {};
+  int tuned_engine[2][32] = {};  // hm_autotune's choice per (precision, n): 0 none, 1 stage, 2 queue
 };
 QueueCfg &queue_cfg();
+int sweep_engine(int n, int precision);
 
 // Exact-SRE raw sums of several states in one persistent launch (12 <= n <= 21 two-pass
 // states and n <= 11 one-warp states); out_dd per item: [p2_hi, p2_lo, m0_hi, m0_lo, ...].

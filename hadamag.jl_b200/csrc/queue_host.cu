@@ -105,6 +105,7 @@ int run_queue(hm_ctx *c, const QueueItem *items, int nitems, const QReq &q, int 
   if (nmax > 0) {
     int X = cfg.X_set ? cfg.X : cfg.tuned_x[fp64 ? 0 : 1][nmax];
     if (X <= 0) X = (int)std::max<long long>(1, ((long long)cfg.slot_mib << 20) / ((long long)vbytes << (nmax - 1)));
+    while (X & (X - 1)) X &= X - 1;  // a power of two
     slot_elems = (long long)X << (nmax - 1);
   }
   const int K = cfg.K;
@@ -131,8 +132,13 @@ int run_queue(hm_ctx *c, const QueueItem *items, int nitems, const QReq &q, int 
       s.X = 1 << (11 - it.n);
       total += (long long)((len + s.X - 1) / s.X);
     } else {
+      // a power of two (the kernel decodes units with shifts): the slot's capacity, or the
+      // next power of two above a shorter range (its extra X-strings are inactive units)
       const long long xcap = slot_elems >> (it.n - 1);
-      s.X = (int)std::min<long long>(xcap, (long long)len);
+      long long x = 1;
+      while (x < (long long)len && x < xcap) x <<= 1;
+      s.X = (int)x;
+      s.lgX = 63 - __builtin_clzll((unsigned long long)x);
       s.nbatch = (int)((len + s.X - 1) / s.X);
       s.q0 = qnext;
       qnext += s.nbatch;

@@ -25,7 +25,9 @@
 // (conflict-free 16-byte / 8-byte accesses).
 #pragma once
 #include "hm_common.cuh"
+#ifdef HM_TMEM_EXCHANGE
 #include "tmem_transpose.cuh"
+#endif
 
 namespace hm {
 
@@ -66,13 +68,18 @@ __device__ __forceinline__ void transpose_ab(V (&v)[R], V *sm, int lane) {
 }
 
 // ---------------------------------------------------------------------------------
-// Lane <-> register exchanges through tensor memory (tmem_transpose.cuh).  A two-pass unit
-// must move the five element bits held by the lane number into registers once per pass.
-// Through shared memory that is a 32 KB store + load per warp unit on the L1/shared data
-// path, which the ring gathers and stores also use; through TMEM it is three (pass 1) or
-// at most three (pass 2) store/load rounds on the tensor-memory path (measured on B200:
-// about 3x the shared-memory rate, and a separate datapath).  A CTA allocates the columns
-// once; each warp uses its own 32 lanes (warp w of the CTA reaches lanes 32 (w mod 4) ..).
+// Lane <-> register exchanges through tensor memory (tmem_transpose.cuh), compiled only
+// with -DHM_TMEM_EXCHANGE.  A two-pass unit must move the five element bits held by the
+// lane number into registers once per pass.  Through shared memory that is a 32 KB store +
+// load per warp unit on the L1/shared data path, which the ring gathers and stores also
+// use; through TMEM it is three (pass 1) or one to three (pass 2) store/load rounds on the
+// tensor-memory path (about 3x the shared-memory rate on B200, and a separate datapath).
+// Measured on B200 the exchanges give bit-identical results but make the sweep 1.5-1.7x
+// slower: every round is a store, a wait, a load and a wait in series, about 700 cycles
+// per warp, and 8 warps per SM cannot hide three of them per unit.  The product path
+// therefore keeps the shared-memory transposes.  A CTA allocates the columns once; each
+// warp uses its own 32 lanes (warp w of the CTA reaches lanes 32 (w mod 4) ..).
+#ifdef HM_TMEM_EXCHANGE
 template <typename T> struct TmemCols { static constexpr int value = sizeof(T) == 8 ? 128 : 64; };
 
 __device__ __forceinline__ uint32_t tmem_cta_alloc(uint32_t *slot, int ncols) {
@@ -123,6 +130,7 @@ __device__ __forceinline__ void tmem_tile(V (&v)[32], uint32_t ta) {
     if constexpr (F64) tmem_xchg_tile10_f64(v, ta); else tmem_xchg_tile10_f32(v, ta);
   }
 }
+#endif  // HM_TMEM_EXCHANGE
 
 // ---------------------------------------------------------------------------------
 // element builders
@@ -402,12 +410,17 @@ __device__ __forceinline__ void p1_unit_tma(const V *__restrict__ psi, const XIn
   V v[R];
   p1_build<R, false>(v, psi, xi, rho, sm, lane);
   reg_wht<R, 0, LOGR>(v);
+#ifdef HM_TMEM_EXCHANGE
   if constexpr (TM) {
     static_assert(R == 32, "the TMEM exchanges are generated for 32 values per lane");
     tmem_row(v, ta);
   } else {
     transpose_ab<R>(v, sm, lane);
   }
+#else
+  (void)ta;
+  transpose_ab<R>(v, sm, lane);
+#endif
   reg_wht<R, 0, 5>(v);
   // register i of lane l holds element k = R l + i, kept at position p = 32 i + l
 #pragma unroll
@@ -429,6 +442,7 @@ __device__ __forceinline__ void p1_unit_tma(const V *__restrict__ psi, const XIn
 template <int R, int HI, int QS, bool TM = false, typename V>
 __device__ __forceinline__ void p2_unit(const V *__restrict__ tile_ptr, V *sm, int lane, double *s,
                                         const QParams &qp, uint32_t ta = 0) {
+  (void)ta;
   constexpr int LOGR = ilog2c(R), PB = LOGR + 5, LOGC = PB - HI;
   static_assert(HI >= 1 && HI <= PB, "pass-2 bits out of range");
   V v[R];
@@ -436,10 +450,12 @@ __device__ __forceinline__ void p2_unit(const V *__restrict__ tile_ptr, V *sm, i
   for (int i = 0; i < R; ++i) v[i] = __ldcg(tile_ptr + i * 32 + lane);
   if constexpr (LOGC >= 5) {
     reg_wht<R, LOGC - 5, LOGR>(v);
+#ifdef HM_TMEM_EXCHANGE
   } else if constexpr (TM && R == 32) {
     reg_wht<R, 0, LOGR>(v);
     tmem_tile<HI>(v, ta);
     reg_wht<R, 0, 5 - LOGC>(v);
+#endif
   } else {
     reg_wht<R, 0, LOGR>(v);
     transpose_ab<R>(v, sm, lane);

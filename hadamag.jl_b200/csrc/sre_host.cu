@@ -140,6 +140,17 @@ static int choose_qs(const QReq &q, QParams &qp, int *idx) {
 
 int queue_choose_qs(const QReq &q, QParams &qp, int *idx) { return choose_qs(q, qp, idx); }
 
+// Sweep of one state's two-pass sizes: 1 = stage kernels, 2 = queue sweep.  HM_PARAM_ENGINE
+// forces one; otherwise the choice hm_autotune recorded for (n, precision), else the stage
+// kernels (measured faster for a single large state on B200: 3.99 vs 4.8 us per X-string at
+// n = 20 in FP64).
+int sweep_engine(int n, int precision) {
+  const QueueCfg &qc = queue_cfg();
+  if (qc.engine == 1 || qc.engine == 2) return qc.engine;
+  const int t = (n >= 0 && n < 32) ? qc.tuned_engine[precision == HM_FP32 ? 1 : 0][n] : 0;
+  return t ? t : 1;
+}
+
 // Queue sweep of several states.  In FP32 the x = 0 transform of every state (F = WHT of
 // |psi|^2, whose F(0)^4 = 1 can dominate m) runs in an FP64 launch of its own and is added
 // as a double-double term, as on the stage-kernel path.
@@ -175,7 +186,7 @@ int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, 
     for (int i = 0; i < 2 * (1 + q.nq); ++i) out_dd[i] = 0.0;
     return HM_OK;
   }
-  if (n >= 12 && queue_cfg().engine == 0) {
+  if (n >= 12 && sweep_engine(n, precision) == 2) {
     const QueueItem it{psi_dev, n, kb, ke};
     return run_queue_sre(c, &it, 1, q, precision, out_dd);
   }
@@ -195,8 +206,8 @@ int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, 
     psi_k = c->d_psi32;
   }
   // x = 0 (F = WHT of |psi|^2, whose F(0)^4 = 1 can dominate m) always runs as one FP64
-  // transform through the plain path: the two-pass kernels have no x = 0 build, and the
-  // FP32 kernels would round it
+  // transform of the queue sweep (which builds it in pass 1): the stage kernels have no
+  // x = 0 build, and the FP32 kernels would round it
   const bool split_zero = kb == 0 && ((n - 1) > 10 || precision == HM_FP32);
   const uint64_t kb_main = split_zero ? 1 : kb;
   int nwarps = 0;
@@ -229,11 +240,12 @@ int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, 
     out_dd[3 + 2 * i] = c->h_out[2 * idx[i] + 1];
   }
   if (split_zero) {
-    // x = 0 (F = WHT of |psi|^2) is not part of the two-pass sweep: one FP64 transform
-    // through the plain path, added as a double-double term
+    // x = 0 (F = WHT of |psi|^2) is not part of the stage kernels' sweep: one FP64
+    // transform of the queue sweep, added as a double-double term
     const double ms_main = c->last_ms;
     double z[10];
-    HM_TRY(run_sre_plain(c, psi_dev, n, 0, 1, q, z));
+    const QueueItem zit{psi_dev, n, 0, 1};
+    HM_TRY(run_queue(c, &zit, 1, q, HM_FP64, z));
     c->last_ms += ms_main;
     for (int t = 0; t < 1 + q.nq; ++t) dd_add_host(out_dd + 2 * t, z[2 * t], z[2 * t + 1]);
   }
@@ -252,9 +264,13 @@ static __global__ void k_tune_state(double2 *psi, uint64_t len) {
   }
 }
 
-// Autotuner of the two-pass batch size: time hm_sre_range on `sample` Gray indices
-// (starting at 1024, where the sweep's steady state begins) for X = 1, 2, 4, ... while
-// the ring stays within 1 GiB, keep the fastest, and record it for this (n, precision).
+// Autotuner of the two-pass sweep of one (n, precision): times hm_sre_range on `sample`
+// Gray indices (starting at 1024, where the sweep's steady state begins) for
+//   the stage kernels with X = 1, 2, 4, ... X-strings per stage (ring up to 1 GiB), and
+//   the queue sweep with X = 1, 2, 4, ... X-strings per ring slot (4 slots up to 1 GiB)
+//   at full occupancy and at one CTA per SM,
+// keeps the fastest (kernel time, CUDA events) and records engine, batch size and CTAs per
+// SM for this (n, precision); later calls use them unless a knob forces another choice.
 extern "C" int hm_autotune(hm_ctx *c, int n, int precision, int *best_x, double *best_us_per_x) {
   if (!c) return HM_ERR_ARG;
   c->err.clear();
@@ -268,11 +284,13 @@ extern "C" int hm_autotune(hm_ctx *c, int n, int precision, int *best_x, double 
   k_tune_state<<<c->num_sms * 4, 256, 0, c->stream>>>((double2 *)c->d_psi, len);
   HM_CUDA(c, cudaGetLastError());
   hm::TwoPassCfg &cfg = hm::twopass_cfg();
+  hm::QueueCfg &qc = hm::queue_cfg();
   const hm::TwoPassCfg saved = cfg;
+  const hm::QueueCfg qsaved = qc;
   const int pi = precision == HM_FP64 ? 0 : 1;
   const uint64_t per_x = (len / 2) * (precision == HM_FP64 ? sizeof(double2) : sizeof(float2));
   const uint64_t rows = len / 2 / 1024;  // pass-1 units per X-string
-  // sample: at least 8 batches of the largest candidate and about 4096 pass-1 units
+  // sample: at least 8 batches of the largest candidate and about 8192 pass-1 units
   uint64_t xmax = 1;
   while (xmax < 256 && 2 * (xmax * 2) * per_x <= (1ull << 30)) xmax *= 2;
   uint64_t sample = std::max<uint64_t>(8 * xmax, (8192 + rows - 1) / rows);
@@ -281,31 +299,82 @@ extern "C" int hm_autotune(hm_ctx *c, int n, int precision, int *best_x, double 
   q.nq = 1;
   q.q[0] = 2.0;
   double dd[10], best = 1e300;
-  int bx = 0;
+  int bx = 0, beng = 1, bcps = 0;
   int rc = HM_OK;
+  auto timeit = [&](double *t) {
+    *t = 1e300;
+    for (int rep = 0; rep < 2 && rc == HM_OK; ++rep) {
+      rc = hm::run_sre(c, (const double2 *)c->d_psi, n, 1024, 1024 + sample, q, precision, dd);
+      if (rc == HM_OK && rep > 0) *t = std::min(*t, c->last_ms);
+    }
+  };
+  // stage kernels
+  qc.engine = 1;
   for (uint64_t X = 1; X <= xmax && rc == HM_OK; X *= 2) {
     cfg.X = (int)X;
     cfg.X_set = 1;
     cfg.ring_mib = std::max<int>(saved.ring_mib, (int)((2 * X * per_x + (1 << 20) - 1) >> 20));
-    double t = 1e300;
-    for (int rep = 0; rep < 2 && rc == HM_OK; ++rep) {
-      rc = hm::run_sre(c, (const double2 *)c->d_psi, n, 1024, 1024 + sample, q, precision, dd);
-      if (rc == HM_OK && rep > 0) t = std::min(t, c->last_ms);
-    }
+    double t;
+    timeit(&t);
     if (rc == HM_OK && t < best) {
       best = t;
       bx = (int)X;
+      beng = 1;
+      bcps = 0;
     }
   }
-  // restore the knobs; keep the result in the table
-  int tuned[2][32];
-  memcpy(tuned, cfg.tuned_x, sizeof tuned);
+  cfg.X_set = saved.X_set;
+  cfg.X = saved.X;
+  cfg.ring_mib = saved.ring_mib;
+  // queue sweep (4 slots of X X-strings each)
+  qc.engine = 2;
+  for (int cps = 0; cps <= 1 && rc == HM_OK; ++cps)
+    for (uint64_t X = 1; 4 * X * per_x <= (1ull << 30) && X <= 256 && rc == HM_OK; X *= 2) {
+      qc.X = (int)X;
+      qc.X_set = 1;
+      qc.ctas_per_sm = cps;
+      double t;
+      timeit(&t);
+      if (rc == HM_OK && t < best) {
+        best = t;
+        bx = (int)X;
+        beng = 2;
+        bcps = cps;
+      }
+    }
+  // restore the knobs; keep the results in the tables
+  int tx[2][32], qx[2][32], qcps[2][32], qeng[2][32];
+  memcpy(tx, cfg.tuned_x, sizeof tx);
+  memcpy(qx, qc.tuned_x, sizeof qx);
+  memcpy(qcps, qc.tuned_cps, sizeof qcps);
+  memcpy(qeng, qc.tuned_engine, sizeof qeng);
   cfg = saved;
-  memcpy(cfg.tuned_x, tuned, sizeof tuned);
+  qc = qsaved;
+  memcpy(cfg.tuned_x, tx, sizeof tx);
+  memcpy(qc.tuned_x, qx, sizeof qx);
+  memcpy(qc.tuned_cps, qcps, sizeof qcps);
+  memcpy(qc.tuned_engine, qeng, sizeof qeng);
   if (rc != HM_OK) return rc;
-  cfg.tuned_x[pi][n] = bx;
+  qc.tuned_engine[pi][n] = beng;
+  if (beng == 1) {
+    cfg.tuned_x[pi][n] = bx;
+  } else {
+    qc.tuned_x[pi][n] = bx;
+    qc.tuned_cps[pi][n] = bcps;
+  }
   *best_x = bx;
   *best_us_per_x = best * 1e3 / (double)sample;
+  return HM_OK;
+}
+
+extern "C" int hm_autotune_choice(int n, int precision, int *engine, int *batch, int *ctas_per_sm) {
+  if (!engine || !batch || !ctas_per_sm) return HM_ERR_ARG;
+  if (n < 0 || n >= 32 || (precision != HM_FP64 && precision != HM_FP32)) return HM_ERR_ARG;
+  const int pi = precision == HM_FP64 ? 0 : 1;
+  const hm::QueueCfg &qc = hm::queue_cfg();
+  *engine = qc.tuned_engine[pi][n];
+  *batch = *engine == 2 ? qc.tuned_x[pi][n] : (*engine == 1 ? hm::twopass_cfg().tuned_x[pi][n] : 0);
+  *ctas_per_sm = *engine == 2 ? qc.tuned_cps[pi][n] : 0;
   return HM_OK;
 }
 
@@ -345,7 +414,7 @@ extern "C" int hm_set_param(int param, int value) {
       cfg.adj_x = value;
       return HM_OK;
     case HM_PARAM_ENGINE:
-      if (value < 0 || value > 1) return HM_ERR_ARG;
+      if (value < 0 || value > 2) return HM_ERR_ARG;
       hm::queue_cfg().engine = value;
       return HM_OK;
     case HM_PARAM_QUEUE_SLOTS:

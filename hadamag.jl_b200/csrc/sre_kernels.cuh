@@ -147,10 +147,16 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
   // the base only changes between replays, after every node of the replay has finished
   const long long t = (long long)*(volatile unsigned *)a.stage + a.node;
   if (t > a.nbatch) return;  // padding stages of the last graph replay
+#ifdef HM_TMEM_EXCHANGE
   // TMEM for the lane <-> register exchanges (the whole CTA takes part; no return below)
   __shared__ uint32_t tmem_slot;
   const uint32_t tmem_base = tmem_cta_alloc(&tmem_slot, TmemCols<T>::value);
   const uint32_t ta = tmem_warp_addr(tmem_base);
+  constexpr bool TM = true;
+#else
+  const uint32_t ta = 0;
+  constexpr bool TM = false;
+#endif
   const int gwarp = blockIdx.x * SRE_WARPS + warp;
   const int nwarps = gridDim.x * SRE_WARPS;
   const V *psi = reinterpret_cast<const V *>(a.psi);
@@ -192,13 +198,13 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
     if (!p2) {
       const V *src = xi.sw < 0 ? psi : reinterpret_cast<const V *>(a.psi_sw[xi.sw]);
       if (a.tma)
-        p1_unit_tma<R, HI, true>(src, xi, sub, sm, lane, &a.tmap, a.g, (int)((b & 1) * a.X + xs), ta, pre);
+        p1_unit_tma<R, HI, TM>(src, xi, sub, sm, lane, &a.tmap, a.g, (int)((b & 1) * a.X + xs), ta, pre);
       else
         p1_unit<R, HI, false>(src, xi, sub, inter_x, sm, lane, pre);
     } else {
       double s[NQ + 1];
       wait_prior_grid();
-      p2_unit<R, HI, QS, true>(inter_x + (sub << PB), sm, lane, s, a.qp, ta);
+      p2_unit<R, HI, QS, TM>(inter_x + (sub << PB), sm, lane, s, a.qp, ta);
       // The tile is dead once read (its slot is rewritten by pass 1 two stages later, in
       // another launch): drop its L2 lines without writing them back to DRAM.
       {
@@ -247,7 +253,9 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
   }
   // the ring rows this warp stored are complete before the grid ends
   if (a.tma && lane == 0) bulk_wait_all();
+#ifdef HM_TMEM_EXCHANGE
   tmem_cta_free(tmem_base, TmemCols<T>::value);
+#endif
 }
 
 // ---------------------------------------------------------------------------------

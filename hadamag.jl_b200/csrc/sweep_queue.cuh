@@ -61,7 +61,8 @@ struct QState {
   uint64_t k_begin, k_end;  // Gray range
   long long u0, u1;         // queue units [u0, u1)
   int n;
-  int X;       // two-pass: X-strings per batch; fused: X-strings per unit
+  int X;       // two-pass: X-strings per batch (a power of two); fused: X-strings per unit
+  int lgX;     // log2 X
   int nbatch;  // two-pass batches
   int q0;      // two-pass: global index of batch 0
 };
@@ -138,10 +139,12 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   V *sm = reinterpret_cast<V *>(smem_q) + warp * (32 * R);
   const int gwarp = blockIdx.x * QWARPS + warp;
+#ifdef HM_TMEM_EXCHANGE
   // TMEM for the two-pass units' lane <-> register exchanges
   __shared__ uint32_t tmem_slot;
   const uint32_t tmem_base = tmem_cta_alloc(&tmem_slot, TmemCols<T>::value);
   const uint32_t ta = tmem_warp_addr(tmem_base);
+#endif
   dd acc[NQ + 1];
 #pragma unroll
   for (int t = 0; t <= NQ; ++t) acc[t] = dd{0.0, 0.0};
@@ -187,14 +190,19 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
     dirty = false;
   };
 
+  // Lane 0 keeps the next claim in flight: the atomic is issued one chunk ahead and its
+  // result is read only when the current chunk is done, so its round trip overlaps the
+  // work.  (A claimed chunk is always later than its holder's current unit, so holding it
+  // cannot block the earliest unfinished unit.)
+  unsigned long long claim = 0;
+  if (lane == 0) claim = atomicAdd(a.next, (unsigned long long)a.chunk);
   for (;;) {
     if (u >= uend) {
-      unsigned long long c0 = 0;
-      if (lane == 0) c0 = atomicAdd(a.next, (unsigned long long)a.chunk);
-      c0 = __shfl_sync(0xffffffffu, c0, 0);
+      unsigned long long c0 = __shfl_sync(0xffffffffu, claim, 0);
       u = (long long)c0;
       uend = u + a.chunk < a.total ? u + a.chunk : a.total;
       if (u >= a.total) break;
+      if (lane == 0) claim = atomicAdd(a.next, (unsigned long long)a.chunk);
     }
     while (a.st[si].u1 <= u) {
       if (dirty) flush();
@@ -256,15 +264,16 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
     }
     // ------------------------------------------------------------------ two-pass unit
     const int hi = n - 11;  // row bits of an X-string's intermediate
-    const long long U = (long long)s.X << hi;  // units per pass per batch
+    const int lgU = s.lgX + hi;
+    const long long U = 1ll << lgU;  // units per pass per batch
     int b, pass;
     long long r;
     if (p < U) {
       b = 0, pass = 1, r = p;
     } else {
       const long long p2 = p - U;
-      const int j = (int)(p2 / (2 * U)) + 1;
-      const long long w = p2 - (long long)(j - 1) * 2 * U;
+      const int j = (int)(p2 >> (lgU + 1)) + 1;
+      const long long w = p2 & (2 * U - 1);
       if (j < s.nbatch) {
         b = w < U ? j : j - 1;
         pass = w < U ? 1 : 2;
@@ -275,8 +284,8 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
     }
     const int q = s.q0 + b;
     const int slot = q % a.K;
-    const int xs = (int)(r % s.X);
-    const uint64_t sub = (uint64_t)(r / s.X);
+    const int xs = (int)(r & (s.X - 1));
+    const uint64_t sub = (uint64_t)(r >> s.lgX);
     const uint64_t k = s.k_begin + (uint64_t)b * s.X + xs;
     const bool active = k < s.k_end;
     const int ti = n - 12;
@@ -329,7 +338,11 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
           }
         }
         reg_wht<R, 0, 5>(v);
+#ifdef HM_TMEM_EXCHANGE
         tmem_row(v, ta);
+#else
+        transpose_ab<R>(v, sm, lane);
+#endif
         reg_wht<R, 0, 5>(v);
         if (a.tma[ti]) {
 #pragma unroll
@@ -379,6 +392,7 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
           reg_wht_rt<R>(v, LOGC - 5, 5);
         } else {
           reg_wht<R, 0, 5>(v);
+#ifdef HM_TMEM_EXCHANGE
           switch (hi) {  // warp-uniform
             case 6: tmem_tile<6>(v, ta); break;
             case 7: tmem_tile<7>(v, ta); break;
@@ -387,6 +401,10 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
             default: tmem_tile<10>(v, ta); break;
           }
           reg_wht_rt<R>(v, 0, 5 - LOGC);
+#else
+          transpose_ab<R>(v, sm, lane);
+          reg_wht_rt<R>(v, LOGC, 5);
+#endif
         }
         double sums[NQ + 1];
         lane_moments<R, QS>(v, sums, a.qp, sm, lane);
@@ -406,7 +424,9 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
   announce();
   if (dirty) flush();
   if (lane == 0) bulk_wait_all();
+#ifdef HM_TMEM_EXCHANGE
   tmem_cta_free(tmem_base, TmemCols<T>::value);
+#endif
 }
 
 // fold of every warp's slot of each state, in warp order: out[s][2t], out[s][2t + 1]

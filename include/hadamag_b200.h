@@ -78,9 +78,11 @@ int hm_set_stream(hm_ctx *ctx, void *cuda_stream);
 #define HM_PARAM_UNITS 3
 #define HM_PARAM_GRAPH 4
 #define HM_PARAM_ADJ_BATCH 5
-/* Knobs of the persistent queue sweep, which runs hm_sre_batched and the two-pass sizes
- * (12 <= n <= 21) of the single-state entry points: HM_PARAM_ENGINE 0 = queue sweep
- * (default), 1 = the stage-kernel sweep; HM_PARAM_QUEUE_SLOTS: ring slots (2..64,
+/* Knobs of the persistent queue sweep, which runs hm_sre_batched (and, when chosen, the
+ * two-pass sizes 12 <= n <= 21 of the single-state entry points): HM_PARAM_ENGINE selects
+ * the single-state sweep, 0 = automatic (the engine hm_autotune recorded for that size
+ * and precision, else the stage kernels), 1 = stage kernels, 2 = queue sweep;
+ * HM_PARAM_QUEUE_SLOTS: ring slots (2..64,
  * default 4); HM_PARAM_QUEUE_SLOT_MIB: size of a ring slot when no batch size is set or
  * tuned (1..4096 MiB, default 16); HM_PARAM_QUEUE_CHUNK: work units a warp claims at a
  * time (1..64, default 1); HM_PARAM_QUEUE_CTAS: CTAs per SM (1..32, 0 = as many as fit).
@@ -98,11 +100,17 @@ int hm_set_stream(hm_ctx *ctx, void *cuda_stream);
 int hm_set_param(int param, int value);
 
 /* Autotuner of the two-pass sweep (no reference counterpart): times the sweep of an n-qubit
- * state for batch sizes X = 1, 2, 4, ... (ring up to 1 GiB) on a sample of Gray indices,
- * records the fastest X for this (n, precision) in a process-wide table that later calls
- * use unless HM_PARAM_BATCH is set, and returns it with the measured microseconds per
- * X-string.  12 <= n <= 21, precision HM_FP64 or HM_FP32.  Takes a fraction of a second. */
+ * state on a sample of Gray indices with the stage kernels (X = 1, 2, 4, ... X-strings per
+ * stage) and with the queue sweep (X = 1, 2, 4, ... X-strings per ring slot, at full
+ * occupancy and at one CTA per SM), records the fastest engine, batch size and CTAs per
+ * SM for this (n, precision) in a process-wide table that later calls use unless a knob
+ * forces another choice, and returns the batch size with the measured microseconds per
+ * X-string.  12 <= n <= 21, precision HM_FP64 or HM_FP32.  Takes a second or two. */
 int hm_autotune(hm_ctx *ctx, int n, int precision, int *best_x, double *best_us_per_x);
+
+/* The choice hm_autotune recorded for (n, precision): engine 0 (not tuned), 1 (stage
+ * kernels) or 2 (queue sweep), its batch size, and CTAs per SM (0 = as many as fit). */
+int hm_autotune_choice(int n, int precision, int *engine, int *batch, int *ctas_per_sm);
 
 /* Number of kernels the last call launched on the device (graph nodes included). */
 int hm_last_launch_count(hm_ctx *ctx, long long *count);

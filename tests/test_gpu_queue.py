@@ -29,7 +29,7 @@ def _dd(x):
 
 @pytest.mark.parametrize("n", [12, 13, 14, 15, 16])
 def test_queue_matches_oracle(ctx, hm, oracle, knobs, n):
-    knobs(hm._native.HM_PARAM_ENGINE, 0)
+    knobs(hm._native.HM_PARAM_ENGINE, 2)
     psi = rand_state(1 << n, 700 + n)
     r2 = oracle.sre(psi, 2)[0]
     r3 = oracle.sre(psi, 3)[0]
@@ -48,7 +48,7 @@ def test_queue_matches_stage_kernels(ctx, hm, knobs, n):
     for kb, ke in ranges:
         knobs(hm._native.HM_PARAM_ENGINE, 1)
         p2s, ms = ctx.sre_range(psi, kb, ke, (2.0, 3.0), hm.HM_FP64)
-        knobs(hm._native.HM_PARAM_ENGINE, 0)
+        knobs(hm._native.HM_PARAM_ENGINE, 2)
         p2q, mq = ctx.sre_range(psi, kb, ke, (2.0, 3.0), hm.HM_FP64)
         assert _dd(p2q) == pytest.approx(_dd(p2s), rel=1e-13)
         for i in range(2):
@@ -57,6 +57,7 @@ def test_queue_matches_stage_kernels(ctx, hm, knobs, n):
 
 def test_queue_knobs_do_not_change_the_sums(ctx, hm, knobs):
     N = hm._native
+    knobs(N.HM_PARAM_ENGINE, 2)
     n = 15
     psi = rand_state(1 << n, 77)
     base = ctx.sre_range(psi, 0, 1 << n, (2.0, 3.0), hm.HM_FP64)
@@ -71,7 +72,8 @@ def test_queue_knobs_do_not_change_the_sums(ctx, hm, knobs):
             assert _dd(m[i]) == pytest.approx(_dd(base[1][i]), rel=1e-14), (param, val)
 
 
-def test_queue_repeatable(ctx, hm):
+def test_queue_repeatable(ctx, hm, knobs):
+    knobs(hm._native.HM_PARAM_ENGINE, 2)
     n = 16
     psi = rand_state(1 << n, 5)
     a = ctx.sre_range(psi, 0, 1 << n, (2.0,), hm.HM_FP64)
@@ -110,6 +112,7 @@ def test_queue_wait_that_gives_up_reports_timeout(ctx, hm, knobs):
     returns HM_ERR_TIMEOUT and the context keeps working."""
     n = 13
     psi = rand_state(1 << n, 3)
+    knobs(hm._native.HM_PARAM_ENGINE, 2)
     knobs(hm._native.HM_PARAM_QUEUE_STALL_TEST, 1)
     with pytest.raises(hm.HadaMAGError, match="gave up"):
         ctx.sre(psi, (2.0,), hm.HM_FP64)

@@ -139,7 +139,9 @@ def test_autotune_records_a_batch_size(ctx, hm, oracle):
     for prec in ("fp64", "fp32"):
         x, us = ctx.autotune(n, hm.PRECISIONS[prec])
         assert x >= 1 and (x & (x - 1)) == 0 and us > 0
-        v, _ = ctx.sre(psi, (2.0,), hm.PRECISIONS[prec])  # runs with the tuned batch size
+        eng, bx, cps = hm._native.autotune_choice(n, hm.PRECISIONS[prec])
+        assert eng in (1, 2) and bx == x and cps in (0, 1)
+        v, _ = ctx.sre(psi, (2.0,), hm.PRECISIONS[prec])  # runs with the tuned engine and batch size
         assert v[0] == close(ref, prec)
     with pytest.raises(hm.ArgumentError):
         ctx.autotune(11, hm.HM_FP64)
