@@ -48,6 +48,7 @@ HM_PARAM_QUEUE_SLOT_MIB = 8
 HM_PARAM_QUEUE_CHUNK = 9
 HM_PARAM_QUEUE_CTAS = 10
 HM_PARAM_QUEUE_STALL_TEST = 11
+HM_PARAM_QUEUE_LEAD = 12
 
 
 class ArgumentError(ValueError):

@@ -108,7 +108,7 @@ int run_queue(hm_ctx *c, const QueueItem *items, int nitems, const QReq &q, int 
     while (X & (X - 1)) X &= X - 1;  // a power of two
     slot_elems = (long long)X << (nmax - 1);
   }
-  const int K = cfg.K;
+  const int K = std::max(cfg.K, cfg.lead + 1);
   const int cps = cfg.ctas_per_sm > 0 ? cfg.ctas_per_sm : (nmax > 0 ? cfg.tuned_cps[fp64 ? 0 : 1][nmax] : 0);
   // queue layout
   std::vector<QState> st(nitems);
@@ -202,6 +202,7 @@ int run_queue(hm_ctx *c, const QueueItem *items, int nitems, const QReq &q, int 
   a.chunk = cfg.chunk;
   a.slot_elems = slot_elems;
   a.stall_test = cfg.stall_test;
+  a.lead = cfg.lead;
   a.poll_limit = cfg.stall_test ? 4096 : QWAIT_POLLS;
   if (nmax > 0) {
     HM_TRY(ensure_dev(c, &c->d_inter, &c->inter_cap, (size_t)K * slot_elems * vbytes));

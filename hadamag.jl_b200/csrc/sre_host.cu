@@ -436,6 +436,11 @@ extern "C" int hm_set_param(int param, int value) {
       if (value < 0 || value > 32) return HM_ERR_ARG;
       hm::queue_cfg().ctas_per_sm = value;
       return HM_OK;
+    case HM_PARAM_QUEUE_LEAD:
+      if (value == 0) value = hm::QueueCfg().lead;
+      if (value < 1 || value > 16) return HM_ERR_ARG;
+      hm::queue_cfg().lead = value;
+      return HM_OK;
     case HM_PARAM_QUEUE_STALL_TEST:
       if (value < 0 || value > 1) return HM_ERR_ARG;
       hm::queue_cfg().stall_test = value;

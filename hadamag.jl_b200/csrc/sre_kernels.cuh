@@ -206,7 +206,12 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
       wait_prior_grid();
       p2_unit<R, HI, QS, TM>(inter_x + (sub << PB), sm, lane, s, a.qp, ta);
       // The tile is dead once read (its slot is rewritten by pass 1 two stages later, in
-      // another launch): drop its L2 lines without writing them back to DRAM.
+      // another launch): drop its L2 lines without writing them back to DRAM.  The next
+      // write to the slot comes after griddepcontrol.wait on the launch in between, which
+      // returns once this launch has finished and its memory operations are performed.
+      // Within one launch a discard is NOT ordered by release/acquire on B200: the queue
+      // sweep, whose slots are rewritten inside the same launch, lost data when it
+      // discarded its tiles, so it does not.
       {
         const char *tb = reinterpret_cast<const char *>(inter_x + (sub << PB));
         constexpr int LINES = (int)(32 * R * sizeof(V) / 128);

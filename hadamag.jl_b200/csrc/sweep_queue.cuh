@@ -12,7 +12,9 @@
 //   pass 2  one 1024-element tile of one X-string's intermediate (2^(n-11) rows x C
 //           positions): the n - 11 remaining levels and the moment sums.
 // A two-pass state is cut into batches of X X-strings whose intermediates fill one ring
-// slot; the queue holds P1(0), then P1(b+1) P2(b) for b = 0, 1, ..., then the last P2.
+// slot; with a lead of L batches the queue holds P1(0) .. P1(L-1), then P1(b+L) P2(b) for
+// b = 0, 1, ..., then the last L P2s, so a batch's pass 2 is claimed about L batches after
+// its pass 1.
 // The batches of all states share one global numbering q and the ring's K slots (slot q
 // mod K).  Two counters per batch replace the kernel boundaries of the stage kernels:
 //   done1[q] counts finished pass-1 units: a pass-2 unit of batch q waits until it
@@ -85,6 +87,7 @@ struct QArgs {
   int K;      // ring slots
   int chunk;  // units claimed per atomic
   int poll_limit;  // polls of a batch counter before a wait gives up
+  int lead;        // batches between a batch's pass 1 and its pass 2 in the queue (>= 1)
   int stall_test;  // 1: pass-2 units of batch 0 wait for one unit more than exist (test of the bounded waits)
 };
 
@@ -129,6 +132,12 @@ __device__ __forceinline__ void warp_wait_count(const unsigned *p, unsigned targ
 
 __device__ __forceinline__ void fence_proxy_async_global() { asm volatile("fence.proxy.async.global;" ::: "memory"); }
 
+// counter += v with release semantics: this thread's earlier memory operations are visible
+// to whoever observes the new count with an acquire load (no separate full fence)
+__device__ __forceinline__ void red_release_add(unsigned *p, unsigned v) {
+  asm volatile("red.release.gpu.global.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+
 template <typename T> struct QOcc { static constexpr int value = sizeof(T) == 8 ? 2 : 3; };
 
 template <typename T, int QS>
@@ -158,8 +167,7 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
     if (lane == 0 && pending >= 0) {
       bulk_wait_all();
       fence_proxy_async_global();
-      __threadfence();
-      atomicAdd(a.done1 + pending, 1u);
+      red_release_add(a.done1 + pending, 1u);
     }
     pending = -1;
   };
@@ -266,20 +274,28 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
     const int hi = n - 11;  // row bits of an X-string's intermediate
     const int lgU = s.lgX + hi;
     const long long U = 1ll << lgU;  // units per pass per batch
+    // segments s = 0 .. nbatch + lead - 1 hold P1(s) (s < nbatch) then P2(s - lead)
+    // (s >= lead): zone A = P1 only, zone B = both, zone C = P2 only
     int b, pass;
     long long r;
-    if (p < U) {
-      b = 0, pass = 1, r = p;
-    } else {
-      const long long p2 = p - U;
-      const int j = (int)(p2 >> (lgU + 1)) + 1;
-      const long long w = p2 & (2 * U - 1);
-      if (j < s.nbatch) {
-        b = w < U ? j : j - 1;
+    {
+      const int L = a.lead, nb = s.nbatch;
+      const int za = L < nb ? L : nb;
+      const long long A = (long long)za << lgU;
+      const long long B = (long long)(nb > L ? nb - L : 0) << (lgU + 1);
+      if (p < A) {
+        b = (int)(p >> lgU), pass = 1, r = p & (U - 1);
+      } else if (p < A + B) {
+        const long long p2 = p - A;
+        const int sg = L + (int)(p2 >> (lgU + 1));
+        const long long w = p2 & (2 * U - 1);
         pass = w < U ? 1 : 2;
-        r = w < U ? w : w - U;
+        b = w < U ? sg : sg - L;
+        r = w & (U - 1);
       } else {
-        b = s.nbatch - 1, pass = 2, r = w;
+        const long long p3 = p - A - B;
+        const int sg = (L > nb ? L : nb) + (int)(p3 >> lgU);
+        b = sg - L, pass = 2, r = p3 & (U - 1);
       }
     }
     const int q = s.q0 + b;
@@ -377,7 +393,7 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
         }
       } else {
         announce();
-        if (lane == 0) atomicAdd(a.done1 + q, 1u);
+        if (lane == 0) red_release_add(a.done1 + q, 1u);
       }
     } else {
       announce();
@@ -415,10 +431,7 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
         dirty = true;
       }
       __syncwarp();
-      if (lane == 0) {
-        __threadfence();
-        atomicAdd(a.done2 + q, 1u);
-      }
+      if (lane == 0) red_release_add(a.done2 + q, 1u);
     }
   }
   announce();

@@ -97,6 +97,9 @@ int hm_set_stream(hm_ctx *ctx, void *cuda_stream);
  * thousand polls, and the call returns HM_ERR_TIMEOUT with the context still usable.
  * Value 0 (default) restores normal operation. */
 #define HM_PARAM_QUEUE_STALL_TEST 11
+/* HM_PARAM_QUEUE_LEAD: batches between a batch's pass 1 and its pass 2 in the queue
+ * (1..16, default 2; the ring keeps at least lead + 1 slots). */
+#define HM_PARAM_QUEUE_LEAD 12
 int hm_set_param(int param, int value);
 
 /* Autotuner of the two-pass sweep (no reference counterpart): times the sweep of an n-qubit

@@ -19,7 +19,7 @@ def knobs(hm):
     N = hm._native
     yield set_param
     for p in (N.HM_PARAM_ENGINE, N.HM_PARAM_QUEUE_SLOTS, N.HM_PARAM_QUEUE_SLOT_MIB, N.HM_PARAM_QUEUE_CHUNK,
-              N.HM_PARAM_QUEUE_CTAS, N.HM_PARAM_BATCH, N.HM_PARAM_QUEUE_STALL_TEST):
+              N.HM_PARAM_QUEUE_CTAS, N.HM_PARAM_BATCH, N.HM_PARAM_QUEUE_STALL_TEST, N.HM_PARAM_QUEUE_LEAD):
         set_param(p, 0)
 
 
@@ -63,7 +63,7 @@ def test_queue_knobs_do_not_change_the_sums(ctx, hm, knobs):
     base = ctx.sre_range(psi, 0, 1 << n, (2.0, 3.0), hm.HM_FP64)
     for param, val in ((N.HM_PARAM_QUEUE_SLOTS, 2), (N.HM_PARAM_QUEUE_SLOTS, 9), (N.HM_PARAM_QUEUE_CHUNK, 5),
                        (N.HM_PARAM_QUEUE_CTAS, 1), (N.HM_PARAM_BATCH, 1), (N.HM_PARAM_BATCH, 64),
-                       (N.HM_PARAM_QUEUE_SLOT_MIB, 1)):
+                       (N.HM_PARAM_QUEUE_SLOT_MIB, 1), (N.HM_PARAM_QUEUE_LEAD, 1), (N.HM_PARAM_QUEUE_LEAD, 5)):
         knobs(param, val)
         p2, m = ctx.sre_range(psi, 0, 1 << n, (2.0, 3.0), hm.HM_FP64)
         knobs(param, 0)

@@ -168,3 +168,26 @@ def test_split_gray_tables_match_oracle(ctx, oracle):
             if x.shape[1] > 1:
                 assert np.array_equal(f, [int(np.argmax(x[:, j] != x[:, j + 1])) + 1 for j in range(x.shape[1] - 1)])
         assert np.array_equal(np.concatenate(cols, axis=1), xt)
+
+
+@pytest.mark.parametrize("n,X", [(12, 1), (13, 2), (14, 1), (16, 4)])
+def test_stage_ring_reuse_is_exact(ctx, hm, oracle, n, X):
+    """Pass 2 drops each tile from L2 after reading it, and pass 1 of the stage after next
+    rewrites the slot.  With tiny batches the stages are a few microseconds long, so a
+    late drop would meet the new rows: every repetition must give the same bits, and the
+    value must match the oracle."""
+    N = hm._native
+    psi = rand_state(1 << n, 900 + n)
+    ref = oracle.sre(psi, 2)[0]
+    N.set_param(N.HM_PARAM_ENGINE, 1)
+    N.set_param(N.HM_PARAM_BATCH, X)
+    try:
+        first = ctx.sre_range(psi, 0, 1 << n, (2.0,), hm.HM_FP64)
+        for _ in range(12):
+            again = ctx.sre_range(psi, 0, 1 << n, (2.0,), hm.HM_FP64)
+            assert np.array_equal(again[0], first[0]) and np.array_equal(again[1], first[1])
+        v, _ = ctx.sre(psi, (2.0,), hm.HM_FP64)
+        assert v[0] == close(ref, "fp64")
+    finally:
+        N.set_param(N.HM_PARAM_BATCH, 0)
+        N.set_param(N.HM_PARAM_ENGINE, 0)
