@@ -63,6 +63,11 @@ CONFIGS = {
 }
 
 
+# default timed steps: about a second of timed work or more per configuration, so that
+# the clock sampler (200 ms period) sees the timed region
+DEFAULT_STEPS = {"c1": 200, "c4n14": 300, "c5pure": 40, "c5mixed": 400}
+
+
 def make_state(dim, seed):
     g = np.random.default_rng(seed)
     v = g.normal(size=dim) + 1j * g.normal(size=dim)
@@ -109,6 +114,10 @@ class ClockSampler:
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # the timed region starts once the sampler is producing samples
+            t0 = time.perf_counter()
+            while not self.lines and time.perf_counter() - t0 < 3.0:
+                time.sleep(0.01)
         except OSError:
             self.proc = None
         return self
@@ -609,11 +618,11 @@ def bench_mana(args, cfg, gpu, world, rank, dist):
     extra["mana"] = float(res["v"])
     line = base_line(args, args.config, name, "phase-points/s", value, world, total_ms, "f64", work, extra)
     if cfg["kind"] == "mana_pure":
-        # per X-string: L 3^(L-1) radix-3 butterflies (16 real ops), 3^L gather-multiplies
-        # (6 ops) and 3^L moduli (4 ops + sqrt)
-        ops = (L * 3 ** (L - 1) * 16 + 3 ** L * 10) * float(3 ** L)
+        # per X-string: L 3^(L-1) radix-3 butterflies (12 FP64 ops: 6 add/sub + 6 FMA),
+        # 3^L gather-multiplies (6 ops) and 3^L moduli (4 ops + sqrt)
+        ops = (L * 3 ** (L - 1) * 12 + 3 ** L * 10) * float(3 ** L)
         line["roofline"] = roofline_fp64(ops, total_ms / args.steps, gpu.ctx.probe_fp64_peak(),
-                                         "(16 L 3^(L-1) + 10 3^L) FP64 ops per ternary X-string")
+                                         "(12 L 3^(L-1) + 10 3^L) FP64 ops per ternary X-string")
     else:
         N = cfg["keep"]
         ops = N * 9 ** N * 81 * 8.0
@@ -754,7 +763,9 @@ def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=None,
+                    help="timed steps (default: 3 for the N = 20 and batched configurations; enough "
+                         "steps for about a second of timed work for the short ones)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default=None, choices=["fp64", "fp32"],
@@ -777,6 +788,10 @@ def main():
         return profile_case(args)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
+    if args.steps is None:
+        args.steps = DEFAULT_STEPS.get(args.config, 3) if args.impl == "ours" else 3
+    if args.steps < 1:
+        ap.error("--steps must be >= 1")
     if args.impl == "reference":
         return run_reference(args)
     return run_ours(args)

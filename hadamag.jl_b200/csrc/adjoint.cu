@@ -665,7 +665,10 @@ int launch_adj_stages(hm_ctx *c, const AdjStageArgs &a0, int *nwarps_out) {
   cudaGraphDestroy(graph);
   if (ce != cudaSuccess)
     return set_err(c, HM_ERR_CUDA, "adjoint graph instantiation failed: %s", cudaGetErrorString(ce));
-  for (int s = 0; s < nst && ce == cudaSuccess; s += G) ce = cudaGraphLaunch(exec, c->stream);
+  for (int s = 0; s < nst && ce == cudaSuccess; s += G) {
+    ce = cudaGraphLaunch(exec, c->stream);
+    c->launches += 4 * G + 1;
+  }
   cudaGraphExecDestroy(exec);
   if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "adjoint graph launch failed: %s", cudaGetErrorString(ce));
   *nwarps_out = nw;
@@ -736,6 +739,7 @@ int run_adj_stages(hm_ctx *c, const double2 *psi, int n, int q, double2 *grad, d
   }
   if (r == HM_OK && ng > 1) {
     k_adj_fold_groups<<<c->num_sms * 4, 256, 0, c->stream>>>(grad, a.gpart, ng - 1, len);
+    c->launches += 1;
     HM_CUDA(c, cudaGetLastError());
   }
   return r;
@@ -773,6 +777,7 @@ int run_sre_grad(hm_ctx *c, const double2 *psi, int n, int q, double *m_out, dou
     blocks = (int)(((long long)chunk * a.U + 3) / 4);
     HM_TRY(ensure_dev(c, &c->d_aux2, &c->aux2_cap, 10 * len * sizeof(double2)));
     k_psi_swapped<double2><<<c->num_sms * 8, 256, 0, c->stream>>>(psi, (double2 *)c->d_aux2, n, 10);
+    c->launches += 1;
     for (int j = 0; j < 10; ++j) a.psi_sw[j] = (const double2 *)c->d_aux2 + (size_t)j * len;
   }
   const int nw = blocks * 4;
@@ -838,6 +843,7 @@ int run_sre_grad(hm_ctx *c, const double2 *psi, int n, int q, double *m_out, dou
 #undef HM_ADJP
     }
     k_adj_acc<<<accb, 256, 0, c->stream>>>(a);
+    c->launches += n <= 11 ? 2 : 4;
   }
   HM_CUDA(c, cudaGetLastError());
   if (n >= 12 && len > x_chunked) {
@@ -847,6 +853,7 @@ int run_sre_grad(hm_ctx *c, const double2 *psi, int n, int q, double *m_out, dou
   HM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
   HM_TRY(ensure_dev(c, (void **)&c->d_out, &c->out_cap, sizeof(double) * 16));
   k_adj_finish<<<1, 256, 0, c->stream>>>(grad_dev, len, a.mpart, (int)nslots, c->d_out);
+  c->launches += 1;
   HM_TRY(ensure_host(c, (void **)&c->h_out, &c->h_out_cap, sizeof(double) * 24));
   HM_CUDA(c, cudaMemcpyAsync(c->h_out, c->d_out, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   HM_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -867,6 +874,7 @@ extern "C" int hm_sre_grad(hm_ctx *c, const double *psi, int n, double q, double
   if (!(q == floor(q) && q >= 1.0 && q <= 8.0))
     return hm::set_err(c, HM_ERR_Q, "adjoint: q = %g must be an integer in [1, 8]", q);
   HM_CUDA(c, cudaSetDevice(c->device));
+  c->launches = 0;
   const size_t len = (size_t)1 << n;
   HM_TRY(hm::ensure_dev(c, &c->d_psi, &c->psi_cap, 2 * len * sizeof(double2)));
   double2 *dpsi = (double2 *)c->d_psi, *dgrad = dpsi + len;

@@ -23,8 +23,6 @@ namespace hm {
 
 namespace {
 
-constexpr int MANA_THREADS = 256;
-
 __host__ __device__ inline int ipow3(int e) {
   int r = 1;
   for (int i = 0; i < e; ++i) r *= 3;
@@ -68,54 +66,57 @@ __device__ __forceinline__ void dft3(double2 &a, double2 &b, double2 &c) {
 
 __host__ __device__ constexpr int ipow3c(int e) { return e <= 0 ? 1 : 3 * ipow3c(e - 1); }
 
-// H3 over the ND digits of `nvec` vectors of 3^ND elements stored at sm[v * VS + e], with
-// compile-time strides (the index arithmetic divides by constants).  Digits go in pairs:
-// one thread loads the 9 elements of a radix-9 group, runs both radix-3 stages in
-// registers and stores them back, so a vector crosses shared memory ceil(ND / 2) times.
-template <int ND, int VS>
-__device__ __forceinline__ void h3_smem(double2 *sm, int nvec) {
-  constexpr int LEN = ipow3c(ND);
+// Register blocks of the qutrit transform H3^{(x)ND} of one vector of 3^ND elements
+// (ND <= 6).  T = 3^ND / E threads hold E = min(27, 3^ND) elements each, in two phases
+// separated by one shared-memory exchange:
+//   phase A: digits 0 .. A-1 (A = min(3, ND)); thread t holds e = t E + k in register k;
+//   phase B: digits A .. ND-1 (B = ND - A <= 3); thread t holds e = j + 27 m for the
+//            GB = 27 / 3^B values j = t + T s (s < GB) and m < 3^B, in register s 3^B + m.
+// Every element crosses shared memory once per pass (written after phase A, read for
+// phase B); each thread runs its radix-27 / radix-3^B butterflies in registers.
+template <int ND> struct QBlock {
+  static constexpr int N = ipow3c(ND);
+  static constexpr int E = N >= 27 ? 27 : N;
+  static constexpr int T = N / E;
+  static constexpr int A = ND < 3 ? ND : 3;
+  static constexpr int B = ND - A;
+  static constexpr int MB = ipow3c(B);
+  static constexpr int GB = 27 / MB;
+};
+
+// H3 over one digit of the register index (stride ST = 3^d): register i pairs with
+// i + ST and i + 2 ST when digit d of i is 0 (every index is a compile-time constant
+// after unrolling, so the block stays in registers)
+template <int NREG, int ST>
+__device__ __forceinline__ void h3_digit(double2 (&v)[NREG]) {
 #pragma unroll
-  for (int d = 0; d + 1 < ND; d += 2) {
-    const int step = ipow3c(d);  // constant once the loop is unrolled
-    constexpr int G9 = LEN >= 9 ? LEN / 9 : 1;  // (the loop body only runs when ND >= 2)
-    for (int t = threadIdx.x; t < nvec * G9; t += blockDim.x) {
-      const int v = t / G9, g = t - v * G9;
-      const int blk = g / step, off = g - blk * step;
-      double2 *base = sm + v * VS + blk * 9 * step + off;
-      double2 x[9];
-#pragma unroll
-      for (int k = 0; k < 9; ++k) x[k] = base[k * step];
-#pragma unroll
-      for (int j = 0; j < 3; ++j) dft3(x[3 * j], x[3 * j + 1], x[3 * j + 2]);  // digit d
-#pragma unroll
-      for (int i = 0; i < 3; ++i) dft3(x[i], x[i + 3], x[i + 6]);  // digit d + 1
-#pragma unroll
-      for (int k = 0; k < 9; ++k) base[k * step] = x[k];
-    }
-    __syncthreads();
-  }
-  if constexpr (ND % 2 == 1) {
-    constexpr int step = LEN / 3, G3 = LEN / 3;  // the last digit
-    for (int t = threadIdx.x; t < nvec * G3; t += blockDim.x) {
-      const int v = t / G3, off = t - v * G3;
-      double2 *base = sm + v * VS + off;
-      double2 x0 = base[0], x1 = base[step], x2 = base[2 * step];
-      dft3(x0, x1, x2);
-      base[0] = x0;
-      base[step] = x1;
-      base[2 * step] = x2;
-    }
-    __syncthreads();
-  }
+  for (int i = 0; i < NREG; ++i)
+    if ((i / ST) % 3 == 0 && i + 2 * ST < NREG) dft3(v[i], v[i + ST], v[i + 2 * ST]);
+}
+// H3 over digits 0 .. ND-1 (ND <= 3) of the register index
+template <int NREG, int ND>
+__device__ __forceinline__ void h3_regs(double2 (&v)[NREG]) {
+  static_assert(ND <= 3, "a register block spans at most three digits");
+  if constexpr (ND >= 1) h3_digit<NREG, 1>(v);
+  if constexpr (ND >= 2) h3_digit<NREG, 3>(v);
+  if constexpr (ND >= 3) h3_digit<NREG, 9>(v);
 }
 
-// shape of the two-pass split for L = LO + HI qutrits: rows of 3^LO elements (pass 1),
-// columns of 3^HI (pass 2), about 2048 elements per CTA
+constexpr int MANA_MAX_THREADS = 256;
+
+// shape of the two-pass split for L = LO + HI qutrits: pass 1 transforms rows of
+// RL = 3^LO elements (ROWS rows per CTA), pass 2 columns of RH = 3^HI elements (COLS
+// adjacent columns per CTA, so that a warp's loads cover consecutive columns)
 template <int LO, int HI> struct ManaShape {
+  using QR = QBlock<LO>;
+  using QC = QBlock<HI>;
   static constexpr int RL = ipow3c(LO), RH = ipow3c(HI);
-  static constexpr int ROWS = (2048 / RL < 1) ? 1 : (2048 / RL > RH ? RH : 2048 / RL);
-  static constexpr int COLS = (2048 / RH < 1) ? 1 : (2048 / RH > RL ? RL : 2048 / RH);
+  static constexpr int ROWS = (MANA_MAX_THREADS / QR::T > RH) ? RH : MANA_MAX_THREADS / QR::T;
+  static constexpr int COLS = (MANA_MAX_THREADS / QC::T > RL) ? RL : MANA_MAX_THREADS / QC::T;
+  static constexpr int NT1 = (ROWS * QR::T + 31) / 32 * 32;
+  static constexpr int NT2 = (COLS * QC::T + 31) / 32 * 32;
+  static constexpr size_t SM1 = (QR::B > 0 ? (size_t)ROWS * RL * 16 : 0) + 2 * RL * sizeof(int);
+  static constexpr size_t SM2 = QC::B > 0 ? (size_t)RH * COLS * 16 : 0;
 };
 
 struct ManaArgs {
@@ -126,18 +127,25 @@ struct ManaArgs {
   double invdim;
 };
 
-// pass 1: rows [blockIdx.x * ROWS, ...) of X-string x0 + blockIdx.y
+// pass 1: rows [blockIdx.x * ROWS, ...) of X-string x0 + blockIdx.y: gather + build
+// v(r) = conj psi(r (+) x) psi((-r) (+) x) / 3^L, transform the row digits.  Pass 1 runs
+// the block phases in the other order: phase A takes the HIGH three digits, thread t
+// holding e = t + T k (so a warp's gathers for one k are adjacent elements), and phase B
+// the low B digits in contiguous groups, thread t holding e = m + MB (t + T s).  The row
+// is stored in the threads' order, position p = (s MB + m) T + t for register s MB + m:
+// a fixed permutation of the positions, which pass 2 (columns) and the sum of |W| do not
+// see, and which makes every store instruction of a warp contiguous.
 template <int LO, int HI>
-__global__ void __launch_bounds__(MANA_THREADS, 4) k_mana_p1(ManaArgs a) {
+__global__ void __launch_bounds__(MANA_MAX_THREADS, 2) k_mana_p1(ManaArgs a) {
   using S = ManaShape<LO, HI>;
-  constexpr int RL = S::RL, RH = S::RH, ROWS = S::ROWS;
+  using Q = typename S::QR;
+  constexpr int RL = S::RL, RH = S::RH, ROWS = S::ROWS, E = Q::E, T = Q::T;
   extern __shared__ __align__(16) unsigned char smraw[];
-  double2 *sm = reinterpret_cast<double2 *>(smraw);
-  int *addL = reinterpret_cast<int *>(sm + ROWS * RL);
+  double2 *sm = reinterpret_cast<double2 *>(smraw);  // ROWS x RL (phase-B exchange)
+  int *addL = reinterpret_cast<int *>(smraw + (Q::B > 0 ? (size_t)ROWS * RL * 16 : 0));
   int *negL = addL + RL;
-  int *rowA = negL + RL, *rowB = rowA + ROWS;
   const int xi = blockIdx.y;
-  if (xi >= a.nx) return;
+  if (xi >= a.nx) return;  // uniform across the CTA
   const int x = a.x0 + xi;
   const int xL = x % RL, xH = x / RL;
   const int row0 = blockIdx.x * ROWS;
@@ -146,57 +154,95 @@ __global__ void __launch_bounds__(MANA_THREADS, 4) k_mana_p1(ManaArgs a) {
     addL[e] = tadd(e, xL, LO);
     negL[e] = tnegadd(e, xL, LO);
   }
-  for (int rr = threadIdx.x; rr < nrows; rr += blockDim.x) {
-    rowA[rr] = tadd(row0 + rr, xH, HI) * RL;
-    rowB[rr] = tnegadd(row0 + rr, xH, HI) * RL;
-  }
   __syncthreads();
-  for (int t = threadIdx.x; t < nrows * RL; t += blockDim.x) {
-    const int rr = t / RL, e = t - rr * RL;
-    const double2 p = a.psi[rowA[rr] + addL[e]];
-    double2 q = a.psi[rowB[rr] + negL[e]];
-    q.x *= a.invdim;
-    q.y *= a.invdim;
-    sm[t] = make_double2(p.x * q.x + p.y * q.y, p.x * q.y - p.y * q.x);  // conj(p) * q
+  const int rr = threadIdx.x / T, t = threadIdx.x - rr * T;
+  const bool act = rr < nrows;
+  double2 v[E];
+  if (act) {
+    const int row = row0 + rr;
+    const double2 *pa = a.psi + (size_t)tadd(row, xH, HI) * RL;
+    const double2 *pb = a.psi + (size_t)tnegadd(row, xH, HI) * RL;
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      const int e = t + T * k;  // T = 1 when the row fits one thread (then e = k)
+      const double2 p = pa[addL[e]];
+      double2 q = pb[negL[e]];
+      q.x *= a.invdim;
+      q.y *= a.invdim;
+      v[k] = make_double2(p.x * q.x + p.y * q.y, p.x * q.y - p.y * q.x);  // conj(p) * q
+    }
+    h3_regs<E, Q::A>(v);  // the register digits of k: element digits B .. LO-1
   }
-  __syncthreads();
-  h3_smem<LO, RL>(sm, nrows);
-  double2 *out = a.inter + ((size_t)xi * RH + row0) * RL;
-  for (int t = threadIdx.x; t < nrows * RL; t += blockDim.x) out[t] = sm[t];
+  double2 *out = a.inter + ((size_t)xi * RH + row0 + rr) * RL;
+  if constexpr (Q::B > 0) {
+    if (act) {
+#pragma unroll
+      for (int k = 0; k < E; ++k) sm[rr * RL + t + T * k] = v[k];
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int s = 0; s < Q::GB; ++s)
+#pragma unroll
+        for (int m = 0; m < Q::MB; ++m) v[s * Q::MB + m] = sm[rr * RL + m + Q::MB * (t + T * s)];
+      h3_regs<27, Q::B>(v);  // element digits 0 .. B-1
+#pragma unroll
+      for (int r = 0; r < 27; ++r) out[r * T + t] = v[r];
+    }
+  } else if (act) {
+#pragma unroll
+    for (int k = 0; k < E; ++k) out[k] = v[k];
+  }
 }
 
-// pass 2: columns [blockIdx.x * COLS, ...) of X-string x0 + blockIdx.y; adds the CTA's
-// sum |W| into its double-double slot
+// pass 2: columns [blockIdx.x * COLS, ...) of X-string x0 + blockIdx.y: transform the
+// column digits and add the CTA's sum |W| into its double-double slot
 template <int LO, int HI>
-__global__ void __launch_bounds__(MANA_THREADS, 4) k_mana_p2(ManaArgs a) {
+__global__ void __launch_bounds__(MANA_MAX_THREADS, 2) k_mana_p2(ManaArgs a) {
   using S = ManaShape<LO, HI>;
-  constexpr int RL = S::RL, RH = S::RH, COLS = S::COLS;
+  using Q = typename S::QC;
+  constexpr int RL = S::RL, RH = S::RH, COLS = S::COLS, E = Q::E, T = Q::T;
   extern __shared__ __align__(16) unsigned char smraw[];
-  double2 *sm = reinterpret_cast<double2 *>(smraw);
-  __shared__ double red[MANA_THREADS / 32];
+  double2 *sm = reinterpret_cast<double2 *>(smraw);  // element e of column c at sm[e COLS + c]
+  __shared__ double red[MANA_MAX_THREADS / 32];
   const int xi = blockIdx.y;
   const int c0 = blockIdx.x * COLS;
   const int ncols = min(COLS, RL - c0);
-  const double2 *in = a.inter + (size_t)xi * RH * RL;
-  if (xi < a.nx) {
-    // sm[col * RH + rH]
-    for (int t = threadIdx.x; t < RH * COLS; t += blockDim.x) {
-      const int rH = t / COLS, col = t - rH * COLS;
-      if (col < ncols) sm[col * RH + rH] = in[(size_t)rH * RL + c0 + col];
+  const int t = threadIdx.x / COLS, c = threadIdx.x - t * COLS;
+  const bool act = xi < a.nx && t < T && c < ncols;
+  const double2 *in = a.inter + (size_t)xi * RH * RL + c0 + c;
+  double2 v[E];
+  if (act) {
+#pragma unroll
+    for (int k = 0; k < E; ++k) v[k] = in[(size_t)(t * E + k) * RL];
+    h3_regs<E, Q::A>(v);
+  }
+  if constexpr (Q::B > 0) {
+    if (act) {
+#pragma unroll
+      for (int k = 0; k < E; ++k) sm[(t * E + k) * COLS + c] = v[k];
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int s = 0; s < Q::GB; ++s)
+#pragma unroll
+        for (int m = 0; m < Q::MB; ++m) v[s * Q::MB + m] = sm[(t + T * s + 27 * m) * COLS + c];
+      h3_regs<27, Q::B>(v);
     }
   }
-  __syncthreads();
-  if (xi < a.nx) h3_smem<HI, RH>(sm, ncols);
-  double s = 0.0;
-  if (xi < a.nx)
-    for (int t = threadIdx.x; t < RH * ncols; t += blockDim.x) s += sqrt(fma(sm[t].x, sm[t].x, sm[t].y * sm[t].y));
+  double sum = 0.0;
+  if (act) {
+#pragma unroll
+    for (int k = 0; k < E; ++k) sum += sqrt(fma(v[k].x, v[k].x, v[k].y * v[k].y));
+  }
   // warp sums, then the warps' sums in warp order
-  s = warp_sum(s);
-  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  sum = warp_sum(sum);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sum;
   __syncthreads();
   if (threadIdx.x == 0) {
     double tot = 0.0;
-    for (int w = 0; w < MANA_THREADS / 32; ++w) tot += red[w];
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
     double *slot = a.slots + 2 * ((size_t)blockIdx.y * gridDim.x + blockIdx.x);
     dd acc{slot[0], slot[1]};
     dd_add(acc, tot);
@@ -354,32 +400,43 @@ static int run_mana_pure_t(hm_ctx *c, const double2 *psi, int xb, int xe, double
   ManaArgs a;
   a.psi = psi;
   a.invdim = 1.0 / (double)D;
-  // X-strings per batch: intermediate of at most 32 MiB (L2 resident)
-  int B = (int)std::max<size_t>(1, ((size_t)32 << 20) / ((size_t)D * sizeof(double2)));
-  if (B > D) B = D;
-  HM_TRY(ensure_dev(c, &c->d_inter, &c->inter_cap, (size_t)B * D * sizeof(double2)));
-  a.inter = (double2 *)c->d_inter;
   const int g1 = (S::RH + S::ROWS - 1) / S::ROWS;
   const int g2 = (S::RL + S::COLS - 1) / S::COLS;
+  auto k1 = k_mana_p1<LO, HI>;
+  auto k2 = k_mana_p2<LO, HI>;
+  HM_CUDA(c, cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SM1));
+  HM_CUDA(c, cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)S::SM2));
+  int occ1 = 0, occ2 = 0;
+  HM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ1, k1, S::NT1, S::SM1));
+  HM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, k2, S::NT2, S::SM2));
+  // X-strings per batch: whole waves of pass-1 CTAs (the last wave of a launch would
+  // otherwise run partly empty), with the intermediate within 64 MiB (L2 resident)
+  const int wave = c->num_sms * std::max(1, std::min(occ1, occ2));
+  const size_t per_x = (size_t)D * sizeof(double2);
+  const int bmax = (int)std::max<size_t>(1, ((size_t)64 << 20) / per_x);
+  int B = std::min(bmax, std::max(1, wave / g1));
+  for (int w = 2; (long long)w * wave / g1 <= bmax; ++w) B = (int)((long long)w * wave / g1);
+  if (B > xe - xb) B = xe - xb;
+  if (B > D) B = D;
+  HM_TRY(ensure_dev(c, &c->d_inter, &c->inter_cap, (size_t)B * per_x));
+  a.inter = (double2 *)c->d_inter;
   const size_t nslots = (size_t)g2 * B;
   HM_TRY(ensure_dev(c, (void **)&c->d_partials, &c->partials_cap, nslots * 2 * sizeof(double)));
   HM_CUDA(c, cudaMemsetAsync(c->d_partials, 0, nslots * 2 * sizeof(double), c->stream));
   a.slots = c->d_partials;
-  const size_t sm1 = (size_t)S::ROWS * S::RL * sizeof(double2) + (2 * S::RL + 2 * S::ROWS) * sizeof(int);
-  const size_t sm2 = (size_t)S::COLS * S::RH * sizeof(double2);
-  HM_CUDA(c, cudaFuncSetAttribute(k_mana_p1<LO, HI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm1));
-  HM_CUDA(c, cudaFuncSetAttribute(k_mana_p2<LO, HI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm2));
   HM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
   for (int x0 = xb; x0 < xe; x0 += B) {
     a.x0 = x0;
     a.nx = std::min(B, xe - x0);
-    k_mana_p1<LO, HI><<<dim3(g1, a.nx), MANA_THREADS, sm1, c->stream>>>(a);
-    k_mana_p2<LO, HI><<<dim3(g2, B), MANA_THREADS, sm2, c->stream>>>(a);
+    k1<<<dim3(g1, a.nx), S::NT1, S::SM1, c->stream>>>(a);
+    k2<<<dim3(g2, B), S::NT2, S::SM2, c->stream>>>(a);
+    c->launches += 2;
   }
   HM_CUDA(c, cudaGetLastError());
   HM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
   HM_TRY(ensure_dev(c, (void **)&c->d_out, &c->out_cap, sizeof(double) * 16));
   k_fold_dd<<<1, 256, 0, c->stream>>>(c->d_partials, (int)nslots, c->d_out);
+  c->launches += 1;
   HM_TRY(ensure_host(c, (void **)&c->h_out, &c->h_out_cap, sizeof(double) * 24));
   HM_CUDA(c, cudaMemcpyAsync(c->h_out, c->d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   HM_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -433,6 +490,7 @@ int run_mana_mixed(hm_ctx *c, const double2 *rho, int N, double *sum_dd) {
   HM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
   HM_TRY(ensure_dev(c, (void **)&c->d_out, &c->out_cap, sizeof(double) * 16));
   k_fold_dd<<<1, 256, 0, c->stream>>>(c->d_partials, nb, c->d_out);
+  c->launches += 3 + N;  // vec9(rho), one per leg, the |w| sums, the fold
   HM_TRY(ensure_host(c, (void **)&c->h_out, &c->h_out_cap, sizeof(double) * 24));
   HM_CUDA(c, cudaMemcpyAsync(c->h_out, c->d_out, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   HM_CUDA(c, cudaStreamSynchronize(c->stream));
@@ -454,6 +512,7 @@ int hm_mana_pure(hm_ctx *c, const double *psi, int L, double *out) {
   if (!psi || !out) return hm::set_err(c, HM_ERR_ARG, "null pointer");
   if (L < 1 || L > 12) return hm::set_err(c, HM_ERR_SIZE, "L = %d qutrits outside [1, 12]", L);
   HM_CUDA(c, cudaSetDevice(c->device));
+  c->launches = 0;
   const size_t D = (size_t)hm::ipow3(L);
   HM_TRY(hm::ensure_dev(c, &c->d_psi, &c->psi_cap, D * sizeof(double2)));
   HM_CUDA(c, cudaMemcpyAsync(c->d_psi, psi, D * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
@@ -473,6 +532,7 @@ int hm_mana_pure_range(hm_ctx *c, const double *psi, int L, int64_t x_begin, int
     return hm::set_err(c, HM_ERR_ARG, "X-string range [%lld, %lld) outside [0, %lld)", (long long)x_begin,
                        (long long)x_end, (long long)D);
   HM_CUDA(c, cudaSetDevice(c->device));
+  c->launches = 0;
   HM_TRY(hm::ensure_dev(c, &c->d_psi, &c->psi_cap, (size_t)D * sizeof(double2)));
   HM_CUDA(c, cudaMemcpyAsync(c->d_psi, psi, (size_t)D * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
   return hm::run_mana_pure(c, (const double2 *)c->d_psi, L, (int)x_begin, (int)x_end, sum_dd);
@@ -484,6 +544,7 @@ int hm_mana_mixed(hm_ctx *c, const double *rho, int N, double *out) {
   if (!rho || !out) return hm::set_err(c, HM_ERR_ARG, "null pointer");
   if (N < 1 || N > 8) return hm::set_err(c, HM_ERR_SIZE, "N = %d qutrits outside [1, 8]", N);
   HM_CUDA(c, cudaSetDevice(c->device));
+  c->launches = 0;
   const size_t dim = (size_t)hm::ipow3(N);
   HM_TRY(hm::ensure_dev(c, &c->d_psi, &c->psi_cap, dim * dim * sizeof(double2)));
   HM_CUDA(c, cudaMemcpyAsync(c->d_psi, rho, dim * dim * sizeof(double2), cudaMemcpyHostToDevice, c->stream));

@@ -356,6 +356,7 @@ int run_mc(hm_ctx *c, const double2 *psi, int n, double q, int nbeta_grid, int c
     a.inter = (double2 *)c->d_inter;
     HM_TRY(ensure_dev(c, &c->d_aux2, &c->aux2_cap, 10 * len * sizeof(double2)));
     k_psi_swapped<double2><<<c->num_sms * 8, 256, 0, c->stream>>>(psi, (double2 *)c->d_aux2, n, 10);
+    c->launches += 1;
     for (int j = 0; j < 10; ++j) a.psi_sw[j] = (const double2 *)c->d_aux2 + (size_t)j * len;
   }
   const size_t part_bytes = (size_t)nbeta * (a.U > 0 ? a.U : 1) * 2 * sizeof(double);
@@ -370,6 +371,7 @@ int run_mc(hm_ctx *c, const double2 *psi, int n, double q, int nbeta_grid, int c
   double *d_res = (double *)(base + 256 + nbeta * sizeof(Chain) + part_bytes);
   uint64_t *d_mask = (uint64_t *)(d_res + 1 + 3 * nbeta);
   k_mc_init<<<(nbeta + 127) / 128, 128, 0, c->stream>>>(a);
+  c->launches += 1;
   HM_CUDA(c, cudaGetLastError());
   // capture a block of steps once, replay it
   const int G = 16;
@@ -392,11 +394,13 @@ int run_mc(hm_ctx *c, const double2 *psi, int n, double q, int nbeta_grid, int c
   for (int s = 0; s < nsamples; s += G) {
     ce = cudaGraphLaunch(exec, c->stream);
     if (ce != cudaSuccess) break;
+    c->launches += G * (n <= 11 ? 2 : 3);  // per step: the sweep kernel(s) and the update
   }
   cudaGraphExecDestroy(exec);
   if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "MC graph launch failed: %s", cudaGetErrorString(ce));
   HM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
   k_mc_finish<<<1, 32, 0, c->stream>>>(a, d_res, d_mask);
+  c->launches += 1;
   HM_CUDA(c, cudaGetLastError());
   HM_CUDA(c, cudaMemcpyAsync(out, d_res, (1 + 3 * nbeta) * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
   if (final_mask)
@@ -426,6 +430,7 @@ int mc_chains(hm_ctx *c, const double *psi, int n, double q, int nbeta, int cb, 
   if (nsamples < 1) return set_err(c, HM_ERR_ARG, "nsamples must be >= 1");
   if (!(q >= 1.0 && q <= 16.0)) return set_err(c, HM_ERR_Q, "Renyi index q = %g outside [1, 16]", q);
   HM_CUDA(c, cudaSetDevice(c->device));
+  c->launches = 0;
   const int nch = ce - cb;
   const size_t len = (size_t)1 << n;
   const size_t ns = (size_t)nch * nsamples;

@@ -4,7 +4,8 @@
 // Mirrors the per-rank part of ext/HadaMAGMPICUDAExt.jl:30-99: the rank's X-string range is
 // split into nearly equal contiguous ranges (split_ranges, ext/HadaMAGMPICUDAExt.jl:8-28:
 // the first N mod k parts one longer), one per GPU, each GPU runs its share with its own
-// workspace from its own host thread, and the per-GPU sums are added.  Here each share is
+// workspace from its own host thread (parts listed on the same device share its thread and
+// run in list order), and the per-GPU sums are added.  Here each share is
 // a hm_sre_range_dev call on that device's context and the shares' double-double sums are
 // added in device-list order, so the result does not depend on which GPU finishes first.
 // A caller with several processes (MPI ranks) passes its own rank's range to
@@ -81,10 +82,24 @@ int hm_sre_range_multi(const int *devices, int ndev, const double *psi, int n, u
   const int w = 2 * nq;
   std::vector<double> p2(2 * parts, 0.0), m((size_t)w * parts, 0.0);
   std::vector<int> rcs(parts, HM_OK);
+  // one host thread per distinct device; parts that share a device run one after another
+  // on that device's thread (kernels of one GPU gain nothing from running side by side)
+  std::vector<int> owner(parts, -1);
+  std::vector<std::vector<int>> groups;
+  for (int i = 0; i < parts; ++i) {
+    for (size_t g = 0; g < groups.size(); ++g)
+      if (devices[groups[g][0]] == devices[i]) owner[i] = (int)g;
+    if (owner[i] < 0) {
+      owner[i] = (int)groups.size();
+      groups.emplace_back();
+    }
+    groups[owner[i]].push_back(i);
+  }
   std::vector<std::thread> th;
-  for (int i = 0; i < parts; ++i)
-    th.emplace_back([&, i] {
-      rcs[i] = hm_sre_range(g_multi_ctx[i], psi, n, kb[i], ke[i], qs, nq, precision, &p2[2 * i], &m[(size_t)w * i]);
+  for (size_t g = 0; g < groups.size(); ++g)
+    th.emplace_back([&, g] {
+      for (int i : groups[g])
+        rcs[i] = hm_sre_range(g_multi_ctx[i], psi, n, kb[i], ke[i], qs, nq, precision, &p2[2 * i], &m[(size_t)w * i]);
     });
   for (auto &t : th) t.join();
   for (int i = 0; i < parts; ++i)

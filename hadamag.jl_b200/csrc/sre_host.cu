@@ -388,7 +388,7 @@ extern "C" int hm_set_param(int param, int value) {
         hm::queue_cfg().X_set = 0;
         return HM_OK;
       }
-      if (value < 1 || value > 4096 || (value & (value - 1))) return HM_ERR_ARG;
+      if (value < 1 || value > 4096) return HM_ERR_ARG;
       cfg.X = value;
       cfg.X_set = 1;
       hm::queue_cfg().X = value;

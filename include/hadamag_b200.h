@@ -66,8 +66,8 @@ const char *hm_last_error(hm_ctx *ctx);
 int hm_set_stream(hm_ctx *ctx, void *cuda_stream);
 
 /* Tuning knobs of the exact-SRE two-pass sweep (n >= 12); the autotuner sets them,
- * defaults apply otherwise.  HM_PARAM_BATCH: X-strings per batch (power of two,
- * 1..4096; 0 = derive it from HM_PARAM_UNITS); HM_PARAM_RING: budget of the two-batch
+ * defaults apply otherwise.  HM_PARAM_BATCH: X-strings per batch (1..4096; the
+ * queue sweep rounds it down to a power of two; 0 = derive it from HM_PARAM_UNITS); HM_PARAM_RING: budget of the two-batch
  * intermediate ring in MiB (8..4096; it should stay L2 resident); HM_PARAM_UNITS: warp
  * units per pass the automatic batch size aims for (256..2^20); HM_PARAM_GRAPH: stage
  * kernels captured per CUDA graph (1..1024); HM_PARAM_ADJ_BATCH: X-strings per batch of
@@ -164,7 +164,7 @@ int hm_sre_range_dev(hm_ctx *ctx, const double *psi_dev, int n, uint64_t k_begin
  * contiguous ranges (split_ranges, ext/HadaMAGMPICUDAExt.jl:8-28: the first N mod ndev
  * one longer), devices[i] sweeps range i from its own host thread with its own context,
  * and the double-double sums are added in list order.  A device may appear more than
- * once.  Contexts are created on first use and kept until hm_multi_release().  Calls are
+ * once: its parts then run one after another on its thread.  Contexts are created on first use and kept until hm_multi_release().  Calls are
  * serialised process-wide; errors are described by hm_multi_last_error() (per thread).
  * psi: host pointer; other arguments and results as hm_sre. */
 int hm_sre_multi(const int *devices, int ndev, const double *psi, int n, const double *qs, int nq, int precision,

@@ -28,7 +28,8 @@ def test_library_exports_every_declared_symbol(hm):
 
 def test_set_param_validation(hm):
     lib = hm._native.load_library()
-    assert lib.hm_set_param(hm._native.HM_PARAM_BATCH, 3) == hm._native.HM_ERR_ARG
+    assert lib.hm_set_param(hm._native.HM_PARAM_BATCH, 5000) == hm._native.HM_ERR_ARG
+    assert lib.hm_set_param(hm._native.HM_PARAM_BATCH, 3) == 0
     assert lib.hm_set_param(hm._native.HM_PARAM_RING, 1) == hm._native.HM_ERR_ARG
     assert lib.hm_set_param(99, 1) == hm._native.HM_ERR_ARG
     assert lib.hm_set_param(hm._native.HM_PARAM_BATCH, 4) == 0

@@ -62,7 +62,7 @@ def test_queue_knobs_do_not_change_the_sums(ctx, hm, knobs):
     psi = rand_state(1 << n, 77)
     base = ctx.sre_range(psi, 0, 1 << n, (2.0, 3.0), hm.HM_FP64)
     for param, val in ((N.HM_PARAM_QUEUE_SLOTS, 2), (N.HM_PARAM_QUEUE_SLOTS, 9), (N.HM_PARAM_QUEUE_CHUNK, 5),
-                       (N.HM_PARAM_QUEUE_CTAS, 1), (N.HM_PARAM_BATCH, 1), (N.HM_PARAM_BATCH, 64),
+                       (N.HM_PARAM_QUEUE_CTAS, 1), (N.HM_PARAM_BATCH, 1), (N.HM_PARAM_BATCH, 64), (N.HM_PARAM_BATCH, 6),
                        (N.HM_PARAM_QUEUE_SLOT_MIB, 1), (N.HM_PARAM_QUEUE_LEAD, 1), (N.HM_PARAM_QUEUE_LEAD, 5)):
         knobs(param, val)
         p2, m = ctx.sre_range(psi, 0, 1 << n, (2.0, 3.0), hm.HM_FP64)
@@ -124,8 +124,9 @@ def test_queue_wait_that_gives_up_reports_timeout(ctx, hm, knobs):
 
 
 def test_sre_multi_matches_single_device(hm, ctx):
-    """hm_sre_multi on one GPU listed one, two and three times: the threads, the range split
-    and the double-double combine give the single-call value."""
+    """hm_sre_multi on one GPU listed one, two and three times (separate contexts, run one
+    after another on the device's thread): the range split and the double-double combine
+    give the single-call value."""
     n = 16
     psi = rand_state(1 << n, 61)
     ref, rlost = ctx.sre(psi, (2.0, 3.0), hm.HM_FP64)

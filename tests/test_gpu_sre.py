@@ -170,7 +170,7 @@ def test_split_gray_tables_match_oracle(ctx, oracle):
         assert np.array_equal(np.concatenate(cols, axis=1), xt)
 
 
-@pytest.mark.parametrize("n,X", [(12, 1), (13, 2), (14, 1), (16, 4)])
+@pytest.mark.parametrize("n,X", [(12, 1), (13, 3), (14, 1), (16, 6)])
 def test_stage_ring_reuse_is_exact(ctx, hm, oracle, n, X):
     """Pass 2 drops each tile from L2 after reading it, and pass 1 of the stage after next
     rewrites the slot.  With tiny batches the stages are a few microseconds long, so a
@@ -191,3 +191,16 @@ def test_stage_ring_reuse_is_exact(ctx, hm, oracle, n, X):
     finally:
         N.set_param(N.HM_PARAM_BATCH, 0)
         N.set_param(N.HM_PARAM_ENGINE, 0)
+
+
+def test_plain_path_at_n22_matches_oracle(ctx, hm, oracle):
+    """n = 22 runs only on the plain multi-launch form: Gray sub-ranges against the oracle
+    (x = 0 included), and Parseval's lost norm on the same state."""
+    n = 22
+    psi = rand_state(1 << n, 2222)
+    N = 1 << n
+    for kb, ke in [(0, 6), (N // 2 + 3, N // 2 + 9), (N - 5, N)]:
+        p2r, mr = oracle.sre_sums(psi, 2, kb + 1, ke)
+        p2, m = ctx.sre_range(psi, kb, ke, (2.0,), hm.HM_PLAIN)
+        assert p2.sum() == pytest.approx(p2r, rel=1e-12)
+        assert m.sum() == pytest.approx(mr, rel=1e-12)
