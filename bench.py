@@ -625,9 +625,10 @@ def bench_mana(args, cfg, gpu, world, rank, dist):
                                          "(12 L 3^(L-1) + 10 3^L) FP64 ops per ternary X-string")
     else:
         N = cfg["keep"]
-        ops = N * 9 ** N * 81 * 8.0
+        # per leg every one of the 9^N outputs is a 9-term complex sum
+        ops = N * 9 ** N * 9 * 8.0
         line["roofline"] = roofline_fp64(ops, total_ms / args.steps, gpu.ctx.probe_fp64_peak(),
-                                         "N 9^N 81 complex multiply-adds (8 FP64 ops each)")
+                                         "N 9^N 9 complex multiply-adds (8 FP64 ops each)")
     line["e2e"] = {"value": units * args.steps / (e2e_ms * 1e-3), "unit": "phase-points/s",
                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": 8}
     line["gpu_launches"] = int(launches)

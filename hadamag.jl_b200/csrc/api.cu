@@ -287,16 +287,20 @@ int hm_sre_batched(hm_ctx *c, int nstates, const double *const *psis, const int 
                                c->stream));
     off += len;
   }
-  // states with n <= 21 go through one persistent queue launch (FP32: plus one FP64
-  // launch of every state's x = 0 transform); larger states and the plain selector run
-  // one state per call
+  // states below the split size go through one persistent queue launch (FP32: plus one
+  // FP64 launch of every state's x = 0 transform); from the split size up a state's own
+  // sweep dwarfs a call's fixed cost and the stage kernels are faster per X-string than
+  // the queue (no dead-tile write-back), so those states, n > 21 and the plain selector
+  // run one state per call
   c->launches = 0;
+  const int split_n = hm::queue_cfg().batch_split_n;
+  auto queued = [&](int n) { return precision != HM_PLAIN && n < split_n && n <= 21; };
   std::vector<QueueItem> items;
   std::vector<int> where;
   off = 0;
   for (int s = 0; s < nstates; ++s) {
     const size_t len = (size_t)1 << ns[s];
-    if (precision != HM_PLAIN && ns[s] <= 21) {
+    if (queued(ns[s])) {
       items.push_back(QueueItem{(const double2 *)c->d_psi + off, ns[s], 0, (uint64_t)len});
       where.push_back(s);
     }
@@ -317,7 +321,7 @@ int hm_sre_batched(hm_ctx *c, int nstates, const double *const *psis, const int 
   off = 0;
   for (int s = 0; s < nstates; ++s) {
     const size_t len = (size_t)1 << ns[s];
-    if (!(precision != HM_PLAIN && ns[s] <= 21)) {
+    if (!queued(ns[s])) {
       c->launches = 0;
       HM_TRY(run_sre(c, (const double2 *)c->d_psi + off, ns[s], 0, len, q, precision, dd.data() + (size_t)s * 2 * (1 + nq)));
       total_ms += c->last_ms;

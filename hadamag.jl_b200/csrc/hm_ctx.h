@@ -141,6 +141,7 @@ struct QueueCfg {
   int engine = 0;  // single-state sweeps: 0 automatic, 1 stage kernels, 2 queue sweep
   int stall_test = 0;  // test of the bounded waits (HM_PARAM_QUEUE_STALL_TEST)
   int lead = 2;        // batches between a batch's pass 1 and pass 2 (HM_PARAM_QUEUE_LEAD)
+  int batch_split_n = 15;  // hm_sre_batched: states from this n up run one per call (HM_PARAM_BATCH_SPLIT_N)
   int tuned_x[2][32] = {};
   int tuned_cps[2][32] = {};
   int tuned_engine[2][32] = {};  // hm_autotune's choice per (precision, n): 0 none, 1 stage, 2 queue

@@ -100,6 +100,13 @@ int hm_set_stream(hm_ctx *ctx, void *cuda_stream);
 /* HM_PARAM_QUEUE_LEAD: batches between a batch's pass 1 and its pass 2 in the queue
  * (1..16, default 2; the ring keeps at least lead + 1 slots). */
 #define HM_PARAM_QUEUE_LEAD 12
+/* HM_PARAM_STAGE_PREFETCH: 2 = each pass-2 unit of the stage kernels prefetches the warp's
+ * next tile into L1 and reads its own through L1; 1 or 0 = off (the default). */
+#define HM_PARAM_STAGE_PREFETCH 13
+/* HM_PARAM_BATCH_SPLIT_N: hm_sre_batched runs states with n below this (1..22, default
+ * 15) in one queue launch and the others one state per call (22: every state up to n = 21
+ * in the queue). */
+#define HM_PARAM_BATCH_SPLIT_N 14
 int hm_set_param(int param, int value);
 
 /* Autotuner of the two-pass sweep (no reference counterpart): times the sweep of an n-qubit
@@ -182,10 +189,11 @@ const char *hm_multi_last_error(void);
 /* Destroy the contexts the multi-GPU calls keep. */
 int hm_multi_release(void);
 
-/* Batched exact SRE of many states of possibly different qubit counts in one launch
- * sequence (no reference counterpart; the reference handles one state per call).
- * psis[s] points to 2^ns[s] interleaved complex doubles (host).  For each state s and
- * each q: out_sre[s*nq + i]; out_lost[s]. */
+/* Batched exact SRE of many states of possibly different qubit counts (no reference
+ * counterpart; the reference handles one state per call): one upload of every state, one
+ * persistent queue launch for the states below HM_PARAM_BATCH_SPLIT_N, one call's kernels
+ * per larger state.  psis[s] points to 2^ns[s] interleaved complex doubles (host).  For
+ * each state s and each q: out_sre[s*nq + i]; out_lost[s]. */
 int hm_sre_batched(hm_ctx *ctx, int nstates, const double *const *psis, const int *ns, const double *qs, int nq,
                    int precision, double *out_sre, double *out_lost);
 

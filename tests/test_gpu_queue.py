@@ -19,7 +19,8 @@ def knobs(hm):
     N = hm._native
     yield set_param
     for p in (N.HM_PARAM_ENGINE, N.HM_PARAM_QUEUE_SLOTS, N.HM_PARAM_QUEUE_SLOT_MIB, N.HM_PARAM_QUEUE_CHUNK,
-              N.HM_PARAM_QUEUE_CTAS, N.HM_PARAM_BATCH, N.HM_PARAM_QUEUE_STALL_TEST, N.HM_PARAM_QUEUE_LEAD):
+              N.HM_PARAM_QUEUE_CTAS, N.HM_PARAM_BATCH, N.HM_PARAM_QUEUE_STALL_TEST, N.HM_PARAM_QUEUE_LEAD,
+              N.HM_PARAM_BATCH_SPLIT_N):
         set_param(p, 0)
 
 
@@ -81,14 +82,18 @@ def test_queue_repeatable(ctx, hm, knobs):
     assert np.array_equal(a[0], b[0]) and np.array_equal(a[1], b[1])
 
 
-def test_batched_mixed_sizes_matches_per_state(ctx, hm, oracle):
-    """The C3 shape on a smaller scale: n drawn from 8..18, q = 2 and 3, one launch."""
+@pytest.mark.parametrize("split", [22, 0])
+def test_batched_mixed_sizes_matches_per_state(ctx, hm, oracle, knobs, split):
+    """The C3 shape on a smaller scale: n drawn from 8..18, q = 2 and 3; every state in one
+    queue launch (split 22), or the default split (n >= 15 one state per call)."""
+    knobs(hm._native.HM_PARAM_BATCH_SPLIT_N, split)
     rng = np.random.default_rng(512)
     ns = [int(v) for v in rng.integers(8, 19, size=40)]
     psis = [rand_state(1 << n, 10_000 + i) for i, n in enumerate(ns)]
     for prec, tol, atol in (("fp64", 1e-10, 0.0), ("fp32", 1e-6, 1e-6)):
         vals, lost = ctx.sre_batched(psis, (2.0, 3.0), hm.PRECISIONS[prec])
-        assert ctx.last_launch_count() <= 6  # queue kernel + fold (+ the FP64 x = 0 launch in FP32)
+        if split == 22:
+            assert ctx.last_launch_count() <= 6  # queue kernel + fold (+ the FP64 x = 0 launch in FP32)
         for i, p in enumerate(psis):
             ref, rlost = ctx.sre(p, (2.0, 3.0), hm.HM_FP64)
             assert vals[i, 0] == pytest.approx(ref[0], rel=tol, abs=atol)
