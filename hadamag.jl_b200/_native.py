@@ -49,7 +49,6 @@ HM_PARAM_QUEUE_CHUNK = 9
 HM_PARAM_QUEUE_CTAS = 10
 HM_PARAM_QUEUE_STALL_TEST = 11
 HM_PARAM_QUEUE_LEAD = 12
-HM_PARAM_STAGE_PREFETCH = 13
 HM_PARAM_BATCH_SPLIT_N = 14
 
 

@@ -115,7 +115,11 @@ template <int LO, int HI> struct ManaShape {
   static constexpr int COLS = (MANA_MAX_THREADS / QC::T > RL) ? RL : MANA_MAX_THREADS / QC::T;
   static constexpr int NT1 = (ROWS * QR::T + 31) / 32 * 32;
   static constexpr int NT2 = (COLS * QC::T + 31) / 32 * 32;
-  static constexpr size_t SM1 = (QR::B > 0 ? (size_t)ROWS * RL * 16 : 0) + 2 * RL * sizeof(int);
+  // pass-1 row stride in shared memory: VS = 1 (mod 8) elements, so that the eight
+  // 16-byte accesses of a quarter warp (consecutive threads T rr + t) fall on distinct
+  // bank groups in both phases (T is odd, T^2 = 1 mod 8)
+  static constexpr int VS = RL + ((1 - RL % 8) + 8) % 8;
+  static constexpr size_t SM1 = (QR::B > 0 ? (size_t)ROWS * VS * 16 : 0) + RL * sizeof(int2);
   static constexpr size_t SM2 = QC::B > 0 ? (size_t)RH * COLS * 16 : 0;
 };
 
@@ -141,9 +145,10 @@ __global__ void __launch_bounds__(MANA_MAX_THREADS, 2) k_mana_p1(ManaArgs a) {
   using Q = typename S::QR;
   constexpr int RL = S::RL, RH = S::RH, ROWS = S::ROWS, E = Q::E, T = Q::T;
   extern __shared__ __align__(16) unsigned char smraw[];
-  double2 *sm = reinterpret_cast<double2 *>(smraw);  // ROWS x RL (phase-B exchange)
-  int *addL = reinterpret_cast<int *>(smraw + (Q::B > 0 ? (size_t)ROWS * RL * 16 : 0));
-  int *negL = addL + RL;
+  double2 *sm = reinterpret_cast<double2 *>(smraw);  // ROWS x VS (phase-B exchange)
+  constexpr int VS = S::VS;
+  // per row element e: (e (+) xL, (-e) (+) xL), one 8-byte load per element
+  int2 *addneg = reinterpret_cast<int2 *>(smraw + (Q::B > 0 ? (size_t)ROWS * VS * 16 : 0));
   const int xi = blockIdx.y;
   if (xi >= a.nx) return;  // uniform across the CTA
   const int x = a.x0 + xi;
@@ -151,8 +156,7 @@ __global__ void __launch_bounds__(MANA_MAX_THREADS, 2) k_mana_p1(ManaArgs a) {
   const int row0 = blockIdx.x * ROWS;
   const int nrows = min(ROWS, RH - row0);
   for (int e = threadIdx.x; e < RL; e += blockDim.x) {
-    addL[e] = tadd(e, xL, LO);
-    negL[e] = tnegadd(e, xL, LO);
+    addneg[e] = make_int2(tadd(e, xL, LO), tnegadd(e, xL, LO));
   }
   __syncthreads();
   const int rr = threadIdx.x / T, t = threadIdx.x - rr * T;
@@ -165,8 +169,9 @@ __global__ void __launch_bounds__(MANA_MAX_THREADS, 2) k_mana_p1(ManaArgs a) {
 #pragma unroll
     for (int k = 0; k < E; ++k) {
       const int e = t + T * k;  // T = 1 when the row fits one thread (then e = k)
-      const double2 p = pa[addL[e]];
-      double2 q = pb[negL[e]];
+      const int2 an = addneg[e];
+      const double2 p = pa[an.x];
+      double2 q = pb[an.y];
       q.x *= a.invdim;
       q.y *= a.invdim;
       v[k] = make_double2(p.x * q.x + p.y * q.y, p.x * q.y - p.y * q.x);  // conj(p) * q
@@ -177,14 +182,14 @@ __global__ void __launch_bounds__(MANA_MAX_THREADS, 2) k_mana_p1(ManaArgs a) {
   if constexpr (Q::B > 0) {
     if (act) {
 #pragma unroll
-      for (int k = 0; k < E; ++k) sm[rr * RL + t + T * k] = v[k];
+      for (int k = 0; k < E; ++k) sm[rr * VS + t + T * k] = v[k];
     }
     __syncthreads();
     if (act) {
 #pragma unroll
       for (int s = 0; s < Q::GB; ++s)
 #pragma unroll
-        for (int m = 0; m < Q::MB; ++m) v[s * Q::MB + m] = sm[rr * RL + m + Q::MB * (t + T * s)];
+        for (int m = 0; m < Q::MB; ++m) v[s * Q::MB + m] = sm[rr * VS + m + Q::MB * (t + T * s)];
       h3_regs<27, Q::B>(v);  // element digits 0 .. B-1
 #pragma unroll
       for (int r = 0; r < 27; ++r) out[r * T + t] = v[r];

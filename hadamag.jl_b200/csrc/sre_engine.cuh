@@ -441,18 +441,13 @@ __device__ __forceinline__ void p1_unit_tma(const V *__restrict__ psi, const XIn
 // (one contiguous block); transform over the row bits, then per-lane moments.
 template <int R, int HI, int QS, bool TM = false, typename V>
 __device__ __forceinline__ void p2_unit(const V *__restrict__ tile_ptr, V *sm, int lane, double *s,
-                                        const QParams &qp, uint32_t ta = 0, bool via_l1 = false) {
+                                        const QParams &qp, uint32_t ta = 0) {
   (void)ta;
   constexpr int LOGR = ilog2c(R), PB = LOGR + 5, LOGC = PB - HI;
   static_assert(HI >= 1 && HI <= PB, "pass-2 bits out of range");
   V v[R];
-  if (via_l1) {  // the tile was prefetched into L1 (written by an earlier, finished launch)
 #pragma unroll
-    for (int i = 0; i < R; ++i) v[i] = __ldca(tile_ptr + i * 32 + lane);
-  } else {
-#pragma unroll
-    for (int i = 0; i < R; ++i) v[i] = __ldcg(tile_ptr + i * 32 + lane);
-  }
+  for (int i = 0; i < R; ++i) v[i] = __ldcg(tile_ptr + i * 32 + lane);
   if constexpr (LOGC >= 5) {
     reg_wht<R, LOGC - 5, LOGR>(v);
 #ifdef HM_TMEM_EXCHANGE

@@ -441,10 +441,6 @@ extern "C" int hm_set_param(int param, int value) {
       if (value < 1 || value > 22) return HM_ERR_ARG;
       hm::queue_cfg().batch_split_n = value;
       return HM_OK;
-    case HM_PARAM_STAGE_PREFETCH:
-      if (value < 0 || value > 2) return HM_ERR_ARG;
-      cfg.prefetch = value == 2 ? 1 : 0;
-      return HM_OK;
     case HM_PARAM_QUEUE_LEAD:
       if (value == 0) value = hm::QueueCfg().lead;
       if (value < 1 || value > 16) return HM_ERR_ARG;

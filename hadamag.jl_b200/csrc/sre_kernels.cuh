@@ -124,7 +124,6 @@ struct StageArgs {
   TmaGeom g;
   int n, X, nbatch, tma;
   int node;            // position of this launch in the captured graph
-  int prefetch;        // 1: each pass-2 unit prefetches the warp's next tile into L1
 };
 
 // wait for the preceding grid (programmatic dependent launch); immediate otherwise
@@ -205,25 +204,7 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
     } else {
       double s[NQ + 1];
       wait_prior_grid();
-      if (a.prefetch) {
-        // the warp's next unit, if it is a pass-2 unit of this stage: its tile (written by
-        // the previous launch, which has finished) goes to L1 while this unit runs
-        const long long u2 = u + nwarps;
-        if (u2 < nfirst + n2) {
-          const long long r2 = u2 - nfirst;
-          const int xs2 = (int)(r2 % a.X);
-          const uint64_t sub2 = (uint64_t)(r2 / a.X);
-          if (a.k_begin + (uint64_t)b * a.X + xs2 < a.k_end) {
-            const char *tb2 =
-                reinterpret_cast<const char *>(ring + ((size_t)(b & 1) * a.X + xs2) * xlen + (sub2 << PB));
-            constexpr int LINES = (int)(32 * R * sizeof(V) / 128);
-#pragma unroll
-            for (int ln = lane; ln < LINES; ln += 32)
-              asm volatile("prefetch.global.L1 [%0];" ::"l"(tb2 + (size_t)ln * 128));
-          }
-        }
-      }
-      p2_unit<R, HI, QS, TM>(inter_x + (sub << PB), sm, lane, s, a.qp, ta, a.prefetch != 0);
+      p2_unit<R, HI, QS, TM>(inter_x + (sub << PB), sm, lane, s, a.qp, ta);
       // The tile is dead once read (its slot is rewritten by pass 1 two stages later, in
       // another launch): drop its L2 lines without writing them back to DRAM.  The next
       // write to the slot comes after griddepcontrol.wait on the launch in between, which

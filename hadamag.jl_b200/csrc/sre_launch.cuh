@@ -31,7 +31,6 @@ struct TwoPassCfg {
   int ring_mib = 64;
   int graph_stages = 32;
   int adj_x = 0;  // X-strings per batch of the adjoint stage kernels (0: the default rule)
-  int prefetch = 0;  // pass-2 units prefetch the warp's next tile into L1 (HM_PARAM_STAGE_PREFETCH)
   // batch sizes chosen by hm_autotune, per precision (0 FP64, 1 FP32) and qubit count;
   // 0 = not tuned.  Used when HM_PARAM_BATCH is not set.
   int tuned_x[2][32] = {};
@@ -100,7 +99,6 @@ static int launch_stages(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
   a.k_end = a0.k_end;
   a.qp = a0.qp;
   a.n = a0.n;
-  a.prefetch = cfg.prefetch;
   const uint64_t U = 1ull << HI;
   const uint64_t len = a.k_end - a.k_begin;
   const TwoPassCfg def;

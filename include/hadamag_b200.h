@@ -100,9 +100,6 @@ int hm_set_stream(hm_ctx *ctx, void *cuda_stream);
 /* HM_PARAM_QUEUE_LEAD: batches between a batch's pass 1 and its pass 2 in the queue
  * (1..16, default 2; the ring keeps at least lead + 1 slots). */
 #define HM_PARAM_QUEUE_LEAD 12
-/* HM_PARAM_STAGE_PREFETCH: 2 = each pass-2 unit of the stage kernels prefetches the warp's
- * next tile into L1 and reads its own through L1; 1 or 0 = off (the default). */
-#define HM_PARAM_STAGE_PREFETCH 13
 /* HM_PARAM_BATCH_SPLIT_N: hm_sre_batched runs states with n below this (1..22, default
  * 15) in one queue launch and the others one state per call (22: every state up to n = 21
  * in the queue). */
