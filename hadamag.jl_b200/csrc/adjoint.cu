@@ -310,21 +310,53 @@ __global__ void __launch_bounds__(128) k_adj_p1b(AdjArgs a) {
   }
 }
 
-// grad(u) += sum over the chunk's X-strings of G_x(u) psi(u ^ x)
-__global__ void k_adj_acc(AdjArgs a) {
+// grad(u) += sum over the chunk's X-strings of G_x(u) psi(u ^ x).  A block covers 32
+// consecutive u; its 8 warps take fixed eighths of the chunk's X-strings (4 interleaved
+// sums each, so several loads are in flight), and warp 0 adds the eighths in order: the
+// result does not depend on scheduling.
+constexpr int ACC_SEGS = 8;
+__global__ void __launch_bounds__(32 * ACC_SEGS) k_adj_acc(AdjArgs a) {
+  __shared__ double2 part[ACC_SEGS][32];
   const uint64_t len = 1ull << a.n;
-  for (uint64_t uu = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; uu < len; uu += (uint64_t)gridDim.x * blockDim.x) {
-    double gr = 0.0, gi = 0.0;
-    for (int xi = 0; xi < a.nx; ++xi) {
-      const double2 g = a.G[(size_t)xi * len + uu];
-      const double2 p = __ldg(a.psi + (uu ^ (a.x0 + xi)));
-      gr += g.x * p.x - g.y * p.y;
-      gi += g.x * p.y + g.y * p.x;
+  const int lane = threadIdx.x & 31, seg = threadIdx.x >> 5;
+  const int per = (a.nx + ACC_SEGS - 1) / ACC_SEGS;
+  const int xb = min(a.nx, seg * per), xe = min(a.nx, xb + per);
+  for (uint64_t base = blockIdx.x * 32ull; base < len; base += (uint64_t)gridDim.x * 32ull) {
+    const uint64_t uu = base + lane;
+    double gr[4] = {0.0, 0.0, 0.0, 0.0}, gi[4] = {0.0, 0.0, 0.0, 0.0};
+    if (uu < len) {
+      int xi = xb;
+      for (; xi + 3 < xe; xi += 4) {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          const double2 g = a.G[(size_t)(xi + j) * len + uu];
+          const double2 p = __ldg(a.psi + (uu ^ (a.x0 + xi + j)));
+          gr[j] += g.x * p.x - g.y * p.y;
+          gi[j] += g.x * p.y + g.y * p.x;
+        }
+      }
+      for (; xi < xe; ++xi) {
+        const double2 g = a.G[(size_t)xi * len + uu];
+        const double2 p = __ldg(a.psi + (uu ^ (a.x0 + xi)));
+        gr[0] += g.x * p.x - g.y * p.y;
+        gi[0] += g.x * p.y + g.y * p.x;
+      }
     }
-    double2 o = a.grad[uu];
-    o.x += gr;
-    o.y += gi;
-    a.grad[uu] = o;
+    part[seg][lane] = make_double2((gr[0] + gr[1]) + (gr[2] + gr[3]), (gi[0] + gi[1]) + (gi[2] + gi[3]));
+    __syncthreads();
+    if (seg == 0 && uu < len) {
+      double2 sum = part[0][lane];
+#pragma unroll
+      for (int k = 1; k < ACC_SEGS; ++k) {
+        sum.x += part[k][lane].x;
+        sum.y += part[k][lane].y;
+      }
+      double2 o = a.grad[uu];
+      o.x += sum.x;
+      o.y += sum.y;
+      a.grad[uu] = o;
+    }
+    __syncthreads();
   }
 }
 
@@ -786,7 +818,7 @@ int run_sre_grad(hm_ctx *c, const double2 *psi, int n, int q, double *m_out, dou
   HM_TRY(ensure_dev(c, (void **)&c->d_partials, &c->partials_cap, nslots * sizeof(double) + 64));
   HM_CUDA(c, cudaMemsetAsync(c->d_partials, 0, nslots * sizeof(double), c->stream));
   a.mpart = c->d_partials;
-  const unsigned accb = (unsigned)std::min<uint64_t>((len + 255) / 256, (uint64_t)c->num_sms * 8);
+  const unsigned accb = (unsigned)std::min<uint64_t>((len + 31) / 32, (uint64_t)c->num_sms * 8);
   HM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
   // n >= 12: the chunked kernels cover x < 2^PB (relabelled copies, x = 0); the stage
   // kernels the rest
@@ -842,7 +874,7 @@ int run_sre_grad(hm_ctx *c, const double2 *psi, int n, int q, double *m_out, dou
       }
 #undef HM_ADJP
     }
-    k_adj_acc<<<accb, 256, 0, c->stream>>>(a);
+    k_adj_acc<<<accb, 32 * ACC_SEGS, 0, c->stream>>>(a);
     c->launches += n <= 11 ? 2 : 4;
   }
   HM_CUDA(c, cudaGetLastError());

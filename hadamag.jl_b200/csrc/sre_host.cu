@@ -181,12 +181,12 @@ int run_queue_sre(hm_ctx *c, const QueueItem *items, int nitems, const QReq &q, 
 
 int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, const QReq &q, int precision,
             double *out_dd) {
-  if (precision == HM_PLAIN || n > 21 || n < 1) return run_sre_plain(c, psi_dev, n, kb, ke, q, out_dd);
+  if (precision == HM_PLAIN || n > 24 || n < 1) return run_sre_plain(c, psi_dev, n, kb, ke, q, out_dd);
   if (ke <= kb) {
     for (int i = 0; i < 2 * (1 + q.nq); ++i) out_dd[i] = 0.0;
     return HM_OK;
   }
-  if (n >= 12 && sweep_engine(n, precision) == 2) {
+  if (n >= 12 && n <= 21 && sweep_engine(n, precision) == 2) {
     const QueueItem it{psi_dev, n, kb, ke};
     return run_queue_sre(c, &it, 1, q, precision, out_dd);
   }
@@ -205,10 +205,12 @@ int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, 
     HM_CUDA(c, cudaGetLastError());
     psi_k = c->d_psi32;
   }
-  // x = 0 (F = WHT of |psi|^2, whose F(0)^4 = 1 can dominate m) always runs as one FP64
-  // transform of the queue sweep (which builds it in pass 1): the stage kernels have no
-  // x = 0 build, and the FP32 kernels would round it
-  const bool split_zero = kb == 0 && ((n - 1) > 10 || precision == HM_FP32);
+  // x = 0 (F = WHT of |psi|^2, whose F(0)^4 = 1 can dominate m) always runs in FP64: for
+  // 12 <= n <= 21 as one transform of the queue sweep (the two-pass stage kernels have no
+  // x = 0 build), for n >= 22 inside the three-pass kernels (an FP32 call runs it as an
+  // FP64 call of its own), and never in the FP32 kernels, which would round it
+  const bool three_pass = n >= 22;
+  const bool split_zero = kb == 0 && (three_pass ? precision == HM_FP32 : ((n - 1) > 10 || precision == HM_FP32));
   const uint64_t kb_main = split_zero ? 1 : kb;
   int nwarps = 0;
   HM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
@@ -244,8 +246,12 @@ int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, 
     // transform of the queue sweep, added as a double-double term
     const double ms_main = c->last_ms;
     double z[10];
-    const QueueItem zit{psi_dev, n, 0, 1};
-    HM_TRY(run_queue(c, &zit, 1, q, HM_FP64, z));
+    if (three_pass) {
+      HM_TRY(run_sre(c, psi_dev, n, 0, 1, q, HM_FP64, z));
+    } else {
+      const QueueItem zit{psi_dev, n, 0, 1};
+      HM_TRY(run_queue(c, &zit, 1, q, HM_FP64, z));
+    }
     c->last_ms += ms_main;
     for (int t = 0; t < 1 + q.nq; ++t) dd_add_host(out_dd + 2 * t, z[2 * t], z[2 * t + 1]);
   }

@@ -3,6 +3,7 @@
 #pragma once
 #include "hm_ctx.h"
 #include "sre_kernels.cuh"
+#include "sweep3.cuh"
 
 namespace hm {
 
@@ -197,6 +198,109 @@ static int launch_stages(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
   return HM_OK;
 }
 
+// Three-pass sweep for n = 21 + K (K = 1 .. 3): batch X (HM_PARAM_BATCH, else about 4096
+// units per pass: X = 2 at n = 22, 1 above), ring of three batches, graph replay of
+// programmatically chained stages as launch_stages.
+template <typename T, int R, int K, int QS>
+static int launch_stages3(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
+  using V = typename VT<T>::V;
+  const TwoPassCfg cfg = twopass_cfg();
+  constexpr int PB = ilog2c(R) + 5, NQ = QSet<QS>::NQ;
+  Stage3Args a;
+  memset(&a, 0, sizeof a);
+  a.psi = a0.psi;
+  a.k_begin = a0.k_begin;
+  a.k_end = a0.k_end;
+  a.qp = a0.qp;
+  a.n = a0.n;
+  const uint64_t U = 1ull << (a.n - 11);
+  const uint64_t len = a.k_end - a.k_begin;
+  uint64_t X = cfg.X_set ? (uint64_t)cfg.X : std::max<uint64_t>(1, 4096 / U);
+  if (X > len) X = len;
+  a.X = (int)X;
+  a.nbatch = (int)((len + X - 1) / X);
+  const uint64_t per_x = ((uint64_t)1 << (a.n - 1)) * sizeof(V);
+  HM_TRY(ensure_dev(c, &c->d_inter, &c->inter_cap, 3 * (size_t)X * per_x));
+  a.ring = c->d_inter;
+  {
+    // the ring as 3 X 2^K sub-vectors in the n = 21 layout: rows of C = 1 position,
+    // 1024 rows, 1024 tiles
+    a.g = ring_tma_geom(1, 1 << PB);
+    a.tma = encode_ring_tmap(&a.tmap, a.ring, (int)sizeof(T), 1, 1 << PB, 1 << PB, (int)(3 * X) << K,
+                             ((uint64_t)1 << 20) * sizeof(V), a.g)
+                ? 1
+                : 0;
+  }
+  if (a.k_begin < (1ull << PB)) {
+    const size_t slen = (size_t)1 << a.n;
+    HM_TRY(ensure_dev(c, &c->d_aux2, &c->aux2_cap, (size_t)PB * slen * sizeof(V)));
+    k_psi_swapped<V><<<c->num_sms * 8, 256, 0, c->stream>>>(reinterpret_cast<const V *>(a.psi),
+                                                            reinterpret_cast<V *>(c->d_aux2), a.n, PB);
+    c->launches += 1;
+    HM_CUDA(c, cudaGetLastError());
+    for (int j = 0; j < PB; ++j) a.psi_sw[j] = reinterpret_cast<const V *>(c->d_aux2) + (size_t)j * slen;
+  }
+  const size_t smem = (size_t)SRE_WARPS * 32 * R * sizeof(V);
+  auto kern = k_sre_stage3<T, R, K, QS>;
+  HM_CUDA(c, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int occ = 0;
+  HM_CUDA(c, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, SRE_WARPS * 32, smem));
+  if (occ < 1) occ = 1;
+  const long long units = (long long)X * (long long)U;
+  int blocks = c->num_sms * occ;
+  if ((long long)blocks * SRE_WARPS > units) blocks = (int)((units + SRE_WARPS - 1) / SRE_WARPS);
+  const int nwarps = blocks * SRE_WARPS;
+  HM_TRY(ensure_dev(c, (void **)&c->d_partials, &c->partials_cap, sizeof(double) * 2 * (NQ + 1) * (size_t)nwarps));
+  HM_CUDA(c, cudaMemsetAsync(c->d_partials, 0, sizeof(double) * 2 * (NQ + 1) * (size_t)nwarps, c->stream));
+  a.slots = c->d_partials;
+  HM_TRY(ensure_dev(c, (void **)&c->d_ctrl, &c->ctrl_cap, 4 * sizeof(unsigned)));
+  HM_CUDA(c, cudaMemsetAsync(c->d_ctrl, 0, 4 * sizeof(unsigned), c->stream));
+  a.stage = c->d_ctrl;
+  const int nst = a.nbatch + 2;
+  const int G = std::min(nst, cfg.graph_stages);
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  HM_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  cudaError_t ce = cudaSuccess;
+  for (int s = 0; s < G && ce == cudaSuccess; ++s) {
+    a.node = s;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(blocks);
+    lc.blockDim = dim3(SRE_WARPS * 32);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = at;
+    lc.numAttrs = s > 0 ? 1 : 0;  // node 0 waits for everything before it
+    ce = cudaLaunchKernelEx(&lc, kern, a);
+  }
+  if (ce == cudaSuccess) {
+    k_stage_advance<<<1, 1, 0, c->stream>>>(a.stage, (unsigned)G);
+    ce = cudaGetLastError();
+  }
+  const cudaError_t ce_end = cudaStreamEndCapture(c->stream, &graph);
+  if (ce == cudaSuccess) ce = ce_end;
+  if (ce != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return set_err(c, HM_ERR_CUDA, "three-pass graph capture failed: %s", cudaGetErrorString(ce));
+  }
+  ce = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ce != cudaSuccess)
+    return set_err(c, HM_ERR_CUDA, "three-pass graph instantiation failed: %s", cudaGetErrorString(ce));
+  for (int s = 0; s < nst && ce == cudaSuccess; s += G) {
+    ce = cudaGraphLaunch(exec, c->stream);
+    c->launches += G + 1;
+  }
+  cudaGraphExecDestroy(exec);
+  if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "three-pass graph launch failed: %s", cudaGetErrorString(ce));
+  *nwarps_out = nwarps;
+  return HM_OK;
+}
+
 #define HM_FUSED_CASE(NBv)                                         \
   case NBv:                                                        \
     return launch_fused<T, R, ((NBv) <= PB ? (NBv) : PB), QS>(c, a, nw);
@@ -237,7 +341,15 @@ static int dispatch_sre(hm_ctx *c, const SreArgs &a, int *nw) {
       HM_2P_CASE(8)
       HM_2P_CASE(9)
       HM_2P_CASE(10)
-      HM_2P_CASE(11)
+      case 11:
+        if constexpr (R == 32) return launch_stages3<T, R, 1, QS>(c, a, nw);
+        break;
+      case 12:
+        if constexpr (R == 32) return launch_stages3<T, R, 2, QS>(c, a, nw);
+        break;
+      case 13:
+        if constexpr (R == 32) return launch_stages3<T, R, 3, QS>(c, a, nw);
+        break;
       default:
         break;
     }

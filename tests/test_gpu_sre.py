@@ -193,14 +193,29 @@ def test_stage_ring_reuse_is_exact(ctx, hm, oracle, n, X):
         N.set_param(N.HM_PARAM_ENGINE, 0)
 
 
-def test_plain_path_at_n22_matches_oracle(ctx, hm, oracle):
-    """n = 22 runs only on the plain multi-launch form: Gray sub-ranges against the oracle
-    (x = 0 included), and Parseval's lost norm on the same state."""
-    n = 22
-    psi = rand_state(1 << n, 2222)
+@pytest.mark.parametrize("n", [22, 23, 24])
+def test_three_pass_sweep_matches_oracle(ctx, hm, oracle, n):
+    """n = 22..24 run the three-pass stage kernels: Gray sub-ranges (x = 0 included, more
+    batches than the three ring slots) against the oracle in FP64 and FP32, and against
+    the plain multi-launch form; an odd batch size at n = 22."""
+    psi = rand_state(1 << n, 2200 + n)
     N = 1 << n
-    for kb, ke in [(0, 6), (N // 2 + 3, N // 2 + 9), (N - 5, N)]:
+    w = 9 if n == 22 else 5
+    for kb, ke in [(0, w), (N // 2 + 3, N // 2 + 3 + w), (N - w, N)]:
         p2r, mr = oracle.sre_sums(psi, 2, kb + 1, ke)
-        p2, m = ctx.sre_range(psi, kb, ke, (2.0,), hm.HM_PLAIN)
-        assert p2.sum() == pytest.approx(p2r, rel=1e-12)
-        assert m.sum() == pytest.approx(mr, rel=1e-12)
+        for prec, tol in (("fp64", 1e-12), ("fp32", 1e-6), ("plain", 1e-12)):
+            p2, m = ctx.sre_range(psi, kb, ke, (2.0,), hm.PRECISIONS[prec])
+            assert p2.sum() == pytest.approx(p2r, rel=tol), (kb, prec)
+            assert m.sum() == pytest.approx(mr, rel=tol), (kb, prec)
+    if n == 22:
+        N_ = hm._native
+        N_.set_param(N_.HM_PARAM_BATCH, 3)
+        try:
+            p2, m = ctx.sre_range(psi, 1000, 1011, (2.0, 3.0), hm.HM_FP64)
+        finally:
+            N_.set_param(N_.HM_PARAM_BATCH, 0)
+        p2b, mb = ctx.sre_range(psi, 1000, 1011, (2.0, 3.0), hm.HM_FP64)
+        assert p2.sum() == pytest.approx(p2b.sum(), rel=1e-13)
+        assert np.allclose(m.sum(axis=1), mb.sum(axis=1), rtol=1e-13)
+        p2r, mr = oracle.sre_sums(psi, 3, 1001, 1011)
+        assert mb[1].sum() == pytest.approx(mr, rel=1e-12)
