@@ -141,8 +141,8 @@ int hm_last_kernel_ms(hm_ctx *ctx, double *ms);
  * qs[0..nq), out_sre[i] = -log2(m_q / 2^n) with m_q = sum over x, k of (F_x(k)^2)^q, and
  * out_lost[0] = |1 - p2 / 2^n| with p2 = sum F^2.  As in the reference, for q != 2 the
  * value is (q-1) times the textbook M_q.
- * psi: host pointer, 2^n interleaved complex doubles.  1 <= n <= 24 (n <= 21 on the
- * fused paths; larger n run the HM_PLAIN structure).  1 <= nq <= 4, each q in
+ * psi: host pointer, 2^n interleaved complex doubles.  1 <= n <= 24 (n <= 11 one fused
+ * pass, 12 <= n <= 21 two passes, 22 <= n <= 24 three passes).  1 <= nq <= 4, each q in
  * [1, 16] (non-integer q allowed). */
 int hm_sre(hm_ctx *ctx, const double *psi, int n, const double *qs, int nq, int precision, double *out_sre,
            double *out_lost);
