@@ -657,31 +657,41 @@ int launch_adj_stages(hm_ctx *c, const AdjStageArgs &a0, int *nwarps_out) {
   a.stage = c->d_ctrl;
   const int nst = a.nbatch + 3;
   const int G = std::min(nst, 32);
+  // stage s, kind k: one chained launch (the very first waits for everything before it)
+  auto launch = [&](int s, int kind) {
+    a.node = s;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(kind == 0 ? blocks_g : blocks);
+    lc.blockDim = dim3((kind == 0 ? GRAD_WARPS : ADJ_WARPS) * 32);
+    lc.dynamicSmemBytes = kind == 0 ? 0 : smem;
+    lc.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = at;
+    lc.numAttrs = (s > 0 || kind > 0) ? 1 : 0;
+    switch (kind) {
+      case 0: return cudaLaunchKernelEx(&lc, k_adjs_grad, a);
+      case 1: return cudaLaunchKernelEx(&lc, k_adjs_p1b<HI>, a);
+      case 2: return cudaLaunchKernelEx(&lc, k_adjs_p2f<HI, QA>, a);
+      default: return cudaLaunchKernelEx(&lc, k_adjs_p1<HI>, a);
+    }
+  };
+  cudaError_t ce = cudaSuccess;
+  if (nst <= G) {
+    // a short sweep: direct launches cost less host time than capturing a graph
+    for (int s = 0; s < nst && ce == cudaSuccess; ++s)
+      for (int kind = 0; kind < 4 && ce == cudaSuccess; ++kind) ce = launch(s, kind);
+    c->launches += 4 * nst;
+    if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "adjoint launch failed: %s", cudaGetErrorString(ce));
+    *nwarps_out = nw;
+    return HM_OK;
+  }
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   HM_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  cudaError_t ce = cudaSuccess;
-  for (int s = 0; s < G && ce == cudaSuccess; ++s) {
-    a.node = s;
-    for (int kind = 0; kind < 4 && ce == cudaSuccess; ++kind) {
-      cudaLaunchConfig_t lc = {};
-      lc.gridDim = dim3(kind == 0 ? blocks_g : blocks);
-      lc.blockDim = dim3((kind == 0 ? GRAD_WARPS : ADJ_WARPS) * 32);
-      lc.dynamicSmemBytes = kind == 0 ? 0 : smem;
-      lc.stream = c->stream;
-      cudaLaunchAttribute at[1];
-      at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-      at[0].val.programmaticStreamSerializationAllowed = 1;
-      lc.attrs = at;
-      lc.numAttrs = (s > 0 || kind > 0) ? 1 : 0;  // the first node waits for everything before it
-      switch (kind) {
-        case 0: ce = cudaLaunchKernelEx(&lc, k_adjs_grad, a); break;
-        case 1: ce = cudaLaunchKernelEx(&lc, k_adjs_p1b<HI>, a); break;
-        case 2: ce = cudaLaunchKernelEx(&lc, k_adjs_p2f<HI, QA>, a); break;
-        default: ce = cudaLaunchKernelEx(&lc, k_adjs_p1<HI>, a); break;
-      }
-    }
-  }
+  for (int s = 0; s < G && ce == cudaSuccess; ++s)
+    for (int kind = 0; kind < 4 && ce == cudaSuccess; ++kind) ce = launch(s, kind);
   if (ce == cudaSuccess) {
     k_stage_advance<<<1, 1, 0, c->stream>>>(a.stage, (unsigned)G);
     ce = cudaGetLastError();

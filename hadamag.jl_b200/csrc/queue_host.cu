@@ -221,56 +221,29 @@ int run_queue(hm_ctx *c, const QueueItem *items, int nitems, const QReq &q, int 
         return set_err(c, HM_ERR_CUDA, "queue sweep: tensor map of the n = %d ring could not be encoded", n);
     }
   }
-  // one graph: clears, state table, sweep, fold, read-back
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  HM_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  cudaError_t ce = cudaSuccess;
-  int rc = HM_OK;
+  // clears, state table, sweep, fold, read-back: one stream sequence (a single launch of
+  // the sweep gains nothing from graph capture, whose instantiation costs more host time
+  // than the whole sweep of a small state)
   int nw_launched = 0;
-  do {
-    if ((ce = cudaMemsetAsync(d_done1, 0, 2 * b_cnt + b_head + b_slots, c->stream)) != cudaSuccess) break;
-    if ((ce = cudaMemcpyAsync(d_st, hb, sizeof(QState) * nitems, cudaMemcpyHostToDevice, c->stream)) != cudaSuccess)
-      break;
-    for (int oi = 0; oi < nitems && ce == cudaSuccess; ++oi)
-      if (st[oi].psi32) {
-        k_psi_to_f32<<<c->num_sms * 4, 256, 0, c->stream>>>(st[oi].psi, (float2 *)st[oi].psi32,
-                                                            (uint64_t)1 << st[oi].n);
-        ce = cudaGetLastError();
-      }
-    if (ce != cudaSuccess) break;
-    // external event-record nodes: the events are recorded when the graph runs (a plain
-    // cudaEventRecord during capture only adds a dependency)
-    if ((ce = cudaEventRecordWithFlags(c->ev0, c->stream, cudaEventRecordExternal)) != cudaSuccess) break;
-    rc = fp64 ? launch_kind<double>(c, kind, a, cps, total, &nw_launched)
-              : launch_kind<float>(c, kind, a, cps, total, &nw_launched);
-    if (rc != HM_OK) break;
-    k_queue_fold<<<nitems, 256, 0, c->stream>>>(d_slots, nw_launched, nitems, nsum, d_out);
-    if ((ce = cudaGetLastError()) != cudaSuccess) break;
-    if ((ce = cudaEventRecordWithFlags(c->ev1, c->stream, cudaEventRecordExternal)) != cudaSuccess) break;
-    if ((ce = cudaMemcpyAsync(h_out, d_out, sizeof(double) * 2 * nsum * nitems, cudaMemcpyDeviceToHost, c->stream)) !=
-        cudaSuccess)
-      break;
-    ce = cudaMemcpyAsync(h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream);
-  } while (0);
-  const cudaError_t ce_end = cudaStreamEndCapture(c->stream, &graph);
-  if (rc != HM_OK || ce != cudaSuccess || ce_end != cudaSuccess) {
-    if (graph) cudaGraphDestroy(graph);
-    cudaGetLastError();
-    if (rc != HM_OK) return rc;
-    return set_err(c, HM_ERR_CUDA, "queue sweep graph capture failed: %s",
-                   cudaGetErrorString(ce != cudaSuccess ? ce : ce_end));
-  }
-  if (nw_launched != nwarps) {
-    cudaGraphDestroy(graph);
+  HM_CUDA(c, cudaMemsetAsync(d_done1, 0, 2 * b_cnt + b_head + b_slots, c->stream));
+  HM_CUDA(c, cudaMemcpyAsync(d_st, hb, sizeof(QState) * nitems, cudaMemcpyHostToDevice, c->stream));
+  for (int oi = 0; oi < nitems; ++oi)
+    if (st[oi].psi32) {
+      k_psi_to_f32<<<c->num_sms * 4, 256, 0, c->stream>>>(st[oi].psi, (float2 *)st[oi].psi32,
+                                                          (uint64_t)1 << st[oi].n);
+      c->launches += 1;
+      HM_CUDA(c, cudaGetLastError());
+    }
+  HM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+  HM_TRY(fp64 ? launch_kind<double>(c, kind, a, cps, total, &nw_launched)
+              : launch_kind<float>(c, kind, a, cps, total, &nw_launched));
+  if (nw_launched != nwarps)
     return set_err(c, HM_ERR_CUDA, "queue sweep: launched %d warps, sized the slots for %d", nw_launched, nwarps);
-  }
-  ce = cudaGraphInstantiate(&exec, graph, 0);
-  cudaGraphDestroy(graph);
-  if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "queue sweep graph instantiation failed: %s", cudaGetErrorString(ce));
-  ce = cudaGraphLaunch(exec, c->stream);
-  cudaGraphExecDestroy(exec);
-  if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "queue sweep graph launch failed: %s", cudaGetErrorString(ce));
+  k_queue_fold<<<nitems, 256, 0, c->stream>>>(d_slots, nw_launched, nitems, nsum, d_out);
+  HM_CUDA(c, cudaGetLastError());
+  HM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+  HM_CUDA(c, cudaMemcpyAsync(h_out, d_out, sizeof(double) * 2 * nsum * nitems, cudaMemcpyDeviceToHost, c->stream));
+  HM_CUDA(c, cudaMemcpyAsync(h_err, d_err, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   HM_CUDA(c, cudaStreamSynchronize(c->stream));
   c->launches += 2;
   float ms = 0.f;

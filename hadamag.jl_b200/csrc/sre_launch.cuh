@@ -85,6 +85,62 @@ static int launch_fused(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
   return HM_OK;
 }
 
+// Launch the nst chained stage kernels of a sweep (node s runs stage s).  Up to one graph's
+// worth of stages go out as direct launches: capturing and instantiating a graph costs
+// more host time than it saves there (an n = 12 call is a handful of stages).  Longer
+// sweeps replay a captured graph of G stages, with a one-thread kernel advancing the stage
+// base in device memory after every replay.
+template <typename Kern, typename Args>
+static int run_stage_chain(hm_ctx *c, Kern kern, Args &a, int nst, int blocks, size_t smem, int G,
+                           const char *what) {
+  auto launch = [&](int s) {
+    a.node = s;
+    cudaLaunchConfig_t lc = {};
+    lc.gridDim = dim3(blocks);
+    lc.blockDim = dim3(SRE_WARPS * 32);
+    lc.dynamicSmemBytes = smem;
+    lc.stream = c->stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    lc.attrs = at;
+    lc.numAttrs = s > 0 ? 1 : 0;  // the first stage waits for everything before it
+    return cudaLaunchKernelEx(&lc, kern, a);
+  };
+  cudaError_t ce = cudaSuccess;
+  if (nst <= G) {
+    for (int s = 0; s < nst && ce == cudaSuccess; ++s) ce = launch(s);
+    c->launches += nst;
+    if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "%s launch failed: %s", what, cudaGetErrorString(ce));
+    return HM_OK;
+  }
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  HM_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  for (int s = 0; s < G && ce == cudaSuccess; ++s) ce = launch(s);
+  if (ce == cudaSuccess) {
+    k_stage_advance<<<1, 1, 0, c->stream>>>(a.stage, (unsigned)G);
+    ce = cudaGetLastError();
+  }
+  const cudaError_t ce_end = cudaStreamEndCapture(c->stream, &graph);
+  if (ce == cudaSuccess) ce = ce_end;
+  if (ce != cudaSuccess) {
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    return set_err(c, HM_ERR_CUDA, "%s graph capture failed: %s", what, cudaGetErrorString(ce));
+  }
+  ce = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "%s graph instantiation failed: %s", what, cudaGetErrorString(ce));
+  for (int s = 0; s < nst && ce == cudaSuccess; s += G) {
+    ce = cudaGraphLaunch(exec, c->stream);
+    c->launches += G + 1;
+  }
+  cudaGraphExecDestroy(exec);
+  if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "%s graph launch failed: %s", what, cudaGetErrorString(ce));
+  return HM_OK;
+}
+
 // Stage-kernel two-pass sweep (see k_sre_stage): X-strings per batch sized so that a
 // pass holds about `units_target` warp units, ring of two batches, stages replayed from
 // a captured CUDA graph.
@@ -155,45 +211,7 @@ static int launch_stages(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
   HM_CUDA(c, cudaMemsetAsync(c->d_ctrl, 0, 4 * sizeof(unsigned), c->stream));
   a.stage = c->d_ctrl;
   const int nst = a.nbatch + 1;
-  const int G = std::min(nst, cfg.graph_stages);
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  HM_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  cudaError_t ce = cudaSuccess;
-  for (int s = 0; s < G && ce == cudaSuccess; ++s) {
-    a.node = s;
-    cudaLaunchConfig_t lc = {};
-    lc.gridDim = dim3(blocks);
-    lc.blockDim = dim3(SRE_WARPS * 32);
-    lc.dynamicSmemBytes = smem;
-    lc.stream = c->stream;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    lc.attrs = at;
-    lc.numAttrs = s > 0 ? 1 : 0;  // node 0 waits for everything before it
-    ce = cudaLaunchKernelEx(&lc, kern, a);
-  }
-  if (ce == cudaSuccess) {
-    k_stage_advance<<<1, 1, 0, c->stream>>>(a.stage, (unsigned)G);
-    ce = cudaGetLastError();
-  }
-  const cudaError_t ce_end = cudaStreamEndCapture(c->stream, &graph);
-  if (ce == cudaSuccess) ce = ce_end;
-  if (ce != cudaSuccess) {
-    if (graph) cudaGraphDestroy(graph);
-    cudaGetLastError();
-    return set_err(c, HM_ERR_CUDA, "stage graph capture failed: %s", cudaGetErrorString(ce));
-  }
-  ce = cudaGraphInstantiate(&exec, graph, 0);
-  cudaGraphDestroy(graph);
-  if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "stage graph instantiation failed: %s", cudaGetErrorString(ce));
-  for (int s = 0; s < nst && ce == cudaSuccess; s += G) {
-    ce = cudaGraphLaunch(exec, c->stream);
-    c->launches += G + 1;
-  }
-  cudaGraphExecDestroy(exec);
-  if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "stage graph launch failed: %s", cudaGetErrorString(ce));
+  HM_TRY(run_stage_chain(c, kern, a, nst, blocks, smem, cfg.graph_stages, "stage"));
   *nwarps_out = nwarps;
   return HM_OK;
 }
@@ -257,46 +275,7 @@ static int launch_stages3(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
   HM_CUDA(c, cudaMemsetAsync(c->d_ctrl, 0, 4 * sizeof(unsigned), c->stream));
   a.stage = c->d_ctrl;
   const int nst = a.nbatch + 2;
-  const int G = std::min(nst, cfg.graph_stages);
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  HM_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-  cudaError_t ce = cudaSuccess;
-  for (int s = 0; s < G && ce == cudaSuccess; ++s) {
-    a.node = s;
-    cudaLaunchConfig_t lc = {};
-    lc.gridDim = dim3(blocks);
-    lc.blockDim = dim3(SRE_WARPS * 32);
-    lc.dynamicSmemBytes = smem;
-    lc.stream = c->stream;
-    cudaLaunchAttribute at[1];
-    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
-    at[0].val.programmaticStreamSerializationAllowed = 1;
-    lc.attrs = at;
-    lc.numAttrs = s > 0 ? 1 : 0;  // node 0 waits for everything before it
-    ce = cudaLaunchKernelEx(&lc, kern, a);
-  }
-  if (ce == cudaSuccess) {
-    k_stage_advance<<<1, 1, 0, c->stream>>>(a.stage, (unsigned)G);
-    ce = cudaGetLastError();
-  }
-  const cudaError_t ce_end = cudaStreamEndCapture(c->stream, &graph);
-  if (ce == cudaSuccess) ce = ce_end;
-  if (ce != cudaSuccess) {
-    if (graph) cudaGraphDestroy(graph);
-    cudaGetLastError();
-    return set_err(c, HM_ERR_CUDA, "three-pass graph capture failed: %s", cudaGetErrorString(ce));
-  }
-  ce = cudaGraphInstantiate(&exec, graph, 0);
-  cudaGraphDestroy(graph);
-  if (ce != cudaSuccess)
-    return set_err(c, HM_ERR_CUDA, "three-pass graph instantiation failed: %s", cudaGetErrorString(ce));
-  for (int s = 0; s < nst && ce == cudaSuccess; s += G) {
-    ce = cudaGraphLaunch(exec, c->stream);
-    c->launches += G + 1;
-  }
-  cudaGraphExecDestroy(exec);
-  if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "three-pass graph launch failed: %s", cudaGetErrorString(ce));
+  HM_TRY(run_stage_chain(c, kern, a, nst, blocks, smem, cfg.graph_stages, "three-pass"));
   *nwarps_out = nwarps;
   return HM_OK;
 }
