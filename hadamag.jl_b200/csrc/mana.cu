@@ -119,7 +119,7 @@ template <int LO, int HI> struct ManaShape {
   // 16-byte accesses of a quarter warp (consecutive threads T rr + t) fall on distinct
   // bank groups in both phases (T is odd, T^2 = 1 mod 8)
   static constexpr int VS = RL + ((1 - RL % 8) + 8) % 8;
-  static constexpr size_t SM1 = (QR::B > 0 ? (size_t)ROWS * VS * 16 : 0) + RL * sizeof(int2);
+  static constexpr size_t SM1 = QR::B > 0 ? (size_t)ROWS * VS * 16 : 0;
   static constexpr size_t SM2 = QC::B > 0 ? (size_t)RH * COLS * 16 : 0;
 };
 
@@ -147,18 +147,12 @@ __global__ void __launch_bounds__(MANA_MAX_THREADS, 2) k_mana_p1(ManaArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   double2 *sm = reinterpret_cast<double2 *>(smraw);  // ROWS x VS (phase-B exchange)
   constexpr int VS = S::VS;
-  // per row element e: (e (+) xL, (-e) (+) xL), one 8-byte load per element
-  int2 *addneg = reinterpret_cast<int2 *>(smraw + (Q::B > 0 ? (size_t)ROWS * VS * 16 : 0));
   const int xi = blockIdx.y;
   if (xi >= a.nx) return;  // uniform across the CTA
   const int x = a.x0 + xi;
   const int xL = x % RL, xH = x / RL;
   const int row0 = blockIdx.x * ROWS;
   const int nrows = min(ROWS, RH - row0);
-  for (int e = threadIdx.x; e < RL; e += blockDim.x) {
-    addneg[e] = make_int2(tadd(e, xL, LO), tnegadd(e, xL, LO));
-  }
-  __syncthreads();
   const int rr = threadIdx.x / T, t = threadIdx.x - rr * T;
   const bool act = rr < nrows;
   double2 v[E];
@@ -166,12 +160,28 @@ __global__ void __launch_bounds__(MANA_MAX_THREADS, 2) k_mana_p1(ManaArgs a) {
     const int row = row0 + rr;
     const double2 *pa = a.psi + (size_t)tadd(row, xH, HI) * RL;
     const double2 *pb = a.psi + (size_t)tnegadd(row, xH, HI) * RL;
+    // e = t + T k: the digit-wise e (+) xL and (-e) (+) xL split into the low B digits
+    // (t, once per thread) and the A register digits of k, whose rotations by the digits
+    // of xL are picked per register at compile time (no table, no shared-memory load)
+    const int xlo = xL % T, xhi = xL / T;
+    const int at = tadd(t, xlo, Q::B), nt = tnegadd(t, xlo, Q::B);
+    int ra[3][3], rn[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+      const int h = (xhi / ipow3c(i)) % 3;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        ra[i][c] = ((h + c) % 3) * ipow3c(i) * T;
+        rn[i][c] = ((h + 3 - c) % 3) * ipow3c(i) * T;
+      }
+    }
 #pragma unroll
     for (int k = 0; k < E; ++k) {
-      const int e = t + T * k;  // T = 1 when the row fits one thread (then e = k)
-      const int2 an = addneg[e];
-      const double2 p = pa[an.x];
-      double2 q = pb[an.y];
+      const int k0 = k % 3, k1 = (k / 3) % 3, k2 = (k / 9) % 3;
+      const int ia = at + ra[0][k0] + (Q::A > 1 ? ra[1][k1] : 0) + (Q::A > 2 ? ra[2][k2] : 0);
+      const int in = nt + rn[0][k0] + (Q::A > 1 ? rn[1][k1] : 0) + (Q::A > 2 ? rn[2][k2] : 0);
+      const double2 p = pa[ia];
+      double2 q = pb[in];
       q.x *= a.invdim;
       q.y *= a.invdim;
       v[k] = make_double2(p.x * q.x + p.y * q.y, p.x * q.y - p.y * q.x);  // conj(p) * q

@@ -75,6 +75,19 @@ size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
 int queue_choose_qs(const QReq &q, QParams &qp, int *idx);  // sre_host.cu (choose_qs)
 
+// FP32 copies of the two-pass states (psi32 set in the state table); blockIdx.y = state
+// y0 + blockIdx.y
+static __global__ void k_queue_psi_to_f32(const QState *__restrict__ st, int y0) {
+  const QState s = st[y0 + blockIdx.y];
+  if (!s.psi32) return;
+  float2 *out = const_cast<float2 *>(s.psi32);
+  const uint64_t len = 1ull << s.n;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < len; i += (uint64_t)gridDim.x * blockDim.x) {
+    const double2 v = s.psi[i];
+    out[i] = make_float2((float)v.x, (float)v.y);
+  }
+}
+
 int run_queue(hm_ctx *c, const QueueItem *items, int nitems, const QReq &q, int precision, double *out_dd) {
   if (nitems <= 0) return HM_OK;
   const bool fp64 = precision != HM_FP32;
@@ -227,13 +240,16 @@ int run_queue(hm_ctx *c, const QueueItem *items, int nitems, const QReq &q, int 
   int nw_launched = 0;
   HM_CUDA(c, cudaMemsetAsync(d_done1, 0, 2 * b_cnt + b_head + b_slots, c->stream));
   HM_CUDA(c, cudaMemcpyAsync(d_st, hb, sizeof(QState) * nitems, cudaMemcpyHostToDevice, c->stream));
-  for (int oi = 0; oi < nitems; ++oi)
-    if (st[oi].psi32) {
-      k_psi_to_f32<<<c->num_sms * 4, 256, 0, c->stream>>>(st[oi].psi, (float2 *)st[oi].psi32,
-                                                          (uint64_t)1 << st[oi].n);
+  if (f32_elems) {
+    // every two-pass state's FP32 copy in one launch (a block row per state, 65535 rows
+    // per launch)
+    const unsigned gx = (unsigned)std::max(1, c->num_sms * 4 / std::max(1, nitems));
+    for (int y0 = 0; y0 < nitems; y0 += 65535) {
+      k_queue_psi_to_f32<<<dim3(gx, (unsigned)std::min(65535, nitems - y0)), 256, 0, c->stream>>>(d_st, y0);
       c->launches += 1;
       HM_CUDA(c, cudaGetLastError());
     }
+  }
   HM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
   HM_TRY(fp64 ? launch_kind<double>(c, kind, a, cps, total, &nw_launched)
               : launch_kind<float>(c, kind, a, cps, total, &nw_launched));
