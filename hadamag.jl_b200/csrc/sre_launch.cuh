@@ -30,7 +30,7 @@ struct TwoPassCfg {
   int X_set = 0;
   int units_target = 4096;
   int ring_mib = 64;
-  int graph_stages = 32;
+  int graph_stages = 128;  // stages per captured graph (128: 0.4 % faster than 32 at n = 20)
   int adj_x = 0;  // X-strings per batch of the adjoint stage kernels (0: the default rule)
   // batch sizes chosen by hm_autotune, per precision (0 FP64, 1 FP32) and qubit count;
   // 0 = not tuned.  Used when HM_PARAM_BATCH is not set.
@@ -85,9 +85,9 @@ static int launch_fused(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
   return HM_OK;
 }
 
-// Launch the nst chained stage kernels of a sweep (node s runs stage s).  Up to one graph's
-// worth of stages go out as direct launches: capturing and instantiating a graph costs
-// more host time than it saves there (an n = 12 call is a handful of stages).  Longer
+// Launch the nst chained stage kernels of a sweep (node s runs stage s).  Up to 32 stages
+// go out as direct launches: capturing and instantiating a graph costs more host time
+// than it saves there (an n = 12 call is a handful of stages).  Longer
 // sweeps replay a captured graph of G stages, with a one-thread kernel advancing the stage
 // base in device memory after every replay.
 template <typename Kern, typename Args>
@@ -108,7 +108,8 @@ static int run_stage_chain(hm_ctx *c, Kern kern, Args &a, int nst, int blocks, s
     return cudaLaunchKernelEx(&lc, kern, a);
   };
   cudaError_t ce = cudaSuccess;
-  if (nst <= G) {
+  G = std::min(G, nst);
+  if (nst <= std::min(G, 32)) {
     for (int s = 0; s < nst && ce == cudaSuccess; ++s) ce = launch(s);
     c->launches += nst;
     if (ce != cudaSuccess) return set_err(c, HM_ERR_CUDA, "%s launch failed: %s", what, cudaGetErrorString(ce));
