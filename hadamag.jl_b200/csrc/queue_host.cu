@@ -176,8 +176,16 @@ int run_queue(hm_ctx *c, const QueueItem *items, int nitems, const QReq &q, int 
   int nwarps = 0;
   HM_TRY(fp64 ? warps_kind<double>(c, kind, cps, total, &nwarps)
               : warps_kind<float>(c, kind, cps, total, &nwarps));
-  // device scratch: [state table][done1][done2][head, err][slots][fold out]
-  const size_t b_st = align_up(sizeof(QState) * nitems, 256);
+  // pass-2 units of every global batch: a pass-1 unit reusing slot q mod K waits for
+  // batch q - K, which may belong to another state with another unit count
+  std::vector<unsigned> bunits((size_t)std::max(qnext, 1), 0u);
+  for (int oi = 0; oi < nitems; ++oi)
+    if (st[oi].n >= 12)
+      for (int b = 0; b < st[oi].nbatch; ++b) bunits[(size_t)st[oi].q0 + b] = (unsigned)st[oi].X << (st[oi].n - 11);
+  // device scratch: [state table, batch unit counts][done1][done2][head, err][slots][fold out]
+  const size_t st_bytes = sizeof(QState) * nitems;
+  const size_t tab_bytes = st_bytes + sizeof(unsigned) * bunits.size();
+  const size_t b_st = align_up(tab_bytes, 256);
   const size_t b_cnt = align_up(sizeof(unsigned) * (size_t)std::max(qnext, 1), 256);
   const size_t b_head = 256;
   const size_t b_slots = align_up(sizeof(double) * 2 * nsum * (size_t)nwarps * nitems, 256);
@@ -192,17 +200,19 @@ int run_queue(hm_ctx *c, const QueueItem *items, int nitems, const QReq &q, int 
   int *d_err = (int *)(base + b_st + 2 * b_cnt + 64);
   double *d_slots = (double *)(base + b_st + 2 * b_cnt + b_head);
   double *d_out = (double *)(base + b_st + 2 * b_cnt + b_head + b_slots);
-  // pinned host mirror: [state table][fold out][err]
+  // pinned host mirror: [state table, batch unit counts][fold out][err]
   const size_t h_bytes = b_st + b_out + 256;
   HM_TRY(ensure_host(c, &c->h_pin, &c->h_pin_cap, h_bytes));
   char *hb = (char *)c->h_pin;
-  memcpy(hb, st.data(), sizeof(QState) * nitems);
+  memcpy(hb, st.data(), st_bytes);
+  memcpy(hb + st_bytes, bunits.data(), sizeof(unsigned) * bunits.size());
   double *h_out = (double *)(hb + b_st);
   int *h_err = (int *)(hb + b_st + b_out);
 
   QArgs a;
   memset(&a, 0, sizeof a);
   a.st = d_st;
+  a.bunits = (const unsigned *)(base + st_bytes);
   a.done1 = d_done1;
   a.done2 = d_done2;
   a.next = d_head;
@@ -239,7 +249,7 @@ int run_queue(hm_ctx *c, const QueueItem *items, int nitems, const QReq &q, int 
   // than the whole sweep of a small state)
   int nw_launched = 0;
   HM_CUDA(c, cudaMemsetAsync(d_done1, 0, 2 * b_cnt + b_head + b_slots, c->stream));
-  HM_CUDA(c, cudaMemcpyAsync(d_st, hb, sizeof(QState) * nitems, cudaMemcpyHostToDevice, c->stream));
+  HM_CUDA(c, cudaMemcpyAsync(d_st, hb, tab_bytes, cudaMemcpyHostToDevice, c->stream));
   if (f32_elems) {
     // every two-pass state's FP32 copy in one launch (a block row per state, 65535 rows
     // per launch)

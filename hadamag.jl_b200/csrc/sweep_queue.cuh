@@ -20,7 +20,8 @@
 //   done1[q] counts finished pass-1 units: a pass-2 unit of batch q waits until it
 //            reaches the batch's unit count;
 //   done2[q] counts finished pass-2 units: the first pass-1 unit to reuse the slot (batch
-//            q + K) waits until it reaches the unit count.
+//            q + K) waits until it reaches batch q's unit count (bunits[q]: batch q may
+//            belong to an earlier, larger state than batch q + K).
 // Every wait is on units that sit earlier in the queue, so they were claimed by running
 // warps that never wait on later units: the sweep cannot deadlock.  Each wait still
 // gives up after a bounded number of polls, records it in `err` and carries on (the host
@@ -77,6 +78,7 @@ struct QArgs {
   const QState *st;
   void *ring;
   unsigned *done1, *done2;  // per global batch
+  const unsigned *bunits;    // per global batch: its pass-1 (= pass-2) unit count
   unsigned long long *next;  // queue head
   double *slots;             // [nwarps][nstates][2 (1 + NQ)]
   int *err;                  // 1 after a wait gave up
@@ -310,7 +312,8 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
     if (pass == 1) {
       if (q >= a.K) {
         announce();
-        warp_wait_count(a.done2 + (q - a.K), (unsigned)U, a.err, lane, a.poll_limit);
+        // batch q - K may belong to an earlier state, with its own unit count
+        warp_wait_count(a.done2 + (q - a.K), a.bunits[q - a.K], a.err, lane, a.poll_limit);
         if (lane == 0) fence_proxy_async_global();  // the slot's reads come before the new stores
       }
       if (active) {

@@ -103,6 +103,25 @@ def test_batched_mixed_sizes_matches_per_state(ctx, hm, oracle, knobs, split):
                 assert vals[i, 0] == pytest.approx(oracle.sre(psis[i], 2)[0], rel=tol, abs=atol)
 
 
+def test_queue_slot_reuse_across_states(ctx, hm, knobs):
+    """A large state followed by smaller ones with small slots and three of them: the
+    first batches of a small state reuse slots of the large state's last batches, whose
+    pass 2 has more units than the small state's.  Every repetition must give the
+    per-state values."""
+    N = hm._native
+    knobs(N.HM_PARAM_BATCH_SPLIT_N, 22)
+    knobs(N.HM_PARAM_QUEUE_SLOT_MIB, 1)
+    knobs(N.HM_PARAM_QUEUE_SLOTS, 3)
+    knobs(N.HM_PARAM_QUEUE_LEAD, 1)
+    ns = [17, 16, 12, 13, 12, 14, 12, 12, 15, 12]
+    psis = [rand_state(1 << n, 4242 + i) for i, n in enumerate(ns)]
+    refs = [ctx.sre(p, (2.0,), hm.HM_FP64)[0][0] for p in psis]
+    for _ in range(6):
+        vals, _ = ctx.sre_batched(psis, (2.0,), hm.HM_FP64)
+        for i in range(len(ns)):
+            assert vals[i, 0] == pytest.approx(refs[i], rel=1e-12), (i, ns[i])
+
+
 def test_batched_generic_q_and_tiny_states(ctx, hm, oracle):
     ns = [1, 2, 5, 11, 12, 13, 3]
     psis = [rand_state(1 << n, 40 + i) for i, n in enumerate(ns)]
