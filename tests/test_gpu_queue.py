@@ -104,22 +104,36 @@ def test_batched_mixed_sizes_matches_per_state(ctx, hm, oracle, knobs, split):
 
 
 def test_queue_slot_reuse_across_states(ctx, hm, knobs):
-    """A large state followed by smaller ones with small slots and three of them: the
-    first batches of a small state reuse slots of the large state's last batches, whose
-    pass 2 has more units than the small state's.  Every repetition must give the
-    per-state values."""
+    """Batches of different unit counts in one launch.  Large slots (256 MiB, three of
+    them): an n = 12 state's single batch holds all its 4096 X-strings (8192 units per
+    pass) while the n >= 13 states fill the slot (16384 units), so the first pass-1 units
+    of an n = 12 state reuse the slot of a larger state's batch, and must wait for all of
+    that batch's pass-2 units, not for as many as their own batch has.  Then FP32, whose
+    x = 0 transforms run as one-X-string batches of 2^(n - 11) units.  Every repetition
+    must give the per-state values."""
     N = hm._native
     knobs(N.HM_PARAM_BATCH_SPLIT_N, 22)
-    knobs(N.HM_PARAM_QUEUE_SLOT_MIB, 1)
+    knobs(N.HM_PARAM_QUEUE_SLOT_MIB, 256)
     knobs(N.HM_PARAM_QUEUE_SLOTS, 3)
     knobs(N.HM_PARAM_QUEUE_LEAD, 1)
-    ns = [17, 16, 12, 13, 12, 14, 12, 12, 15, 12]
+    ns = [16, 12, 13, 12, 14, 12, 12, 13, 12]
     psis = [rand_state(1 << n, 4242 + i) for i, n in enumerate(ns)]
     refs = [ctx.sre(p, (2.0,), hm.HM_FP64)[0][0] for p in psis]
     for _ in range(6):
         vals, _ = ctx.sre_batched(psis, (2.0,), hm.HM_FP64)
         for i in range(len(ns)):
             assert vals[i, 0] == pytest.approx(refs[i], rel=1e-12), (i, ns[i])
+    # FP32: every state's x = 0 transform runs as a one-X-string batch of its own in one
+    # FP64 launch, so consecutive batches there have 2^(n - 11) units each
+    for p in (N.HM_PARAM_QUEUE_SLOT_MIB, N.HM_PARAM_QUEUE_SLOTS, N.HM_PARAM_QUEUE_LEAD):
+        knobs(p, 0)
+    ns = [18, 17, 16, 15, 14, 13, 12, 12, 12, 12, 13, 12]
+    psis = [rand_state(1 << n, 4343 + i) for i, n in enumerate(ns)]
+    refs = [ctx.sre(p, (2.0,), hm.HM_FP64)[0][0] for p in psis]
+    for _ in range(6):
+        vals, _ = ctx.sre_batched(psis, (2.0,), hm.HM_FP32)
+        for i in range(len(ns)):
+            assert vals[i, 0] == pytest.approx(refs[i], rel=1e-6), (i, ns[i])
 
 
 def test_batched_generic_q_and_tiny_states(ctx, hm, oracle):
