@@ -117,12 +117,15 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
   return v;
 }
 
-// lane 0 polls until *p >= target (bounded); the warp then proceeds together
+// lane 0 polls until *p >= target (bounded); the warp then proceeds together.  A wait
+// also gives up as soon as another wait of the launch has given up (every 64 polls it
+// looks at the error word), so a failed launch ends after one poll limit, not one per
+// waiting unit.
 __device__ __forceinline__ void warp_wait_count(const unsigned *p, unsigned target, int *err, int lane, int limit) {
   if (lane == 0) {
     int polls = 0;
     while (ld_acquire(p) < target) {
-      if (++polls >= limit) {
+      if (++polls >= limit || ((polls & 63) == 0 && *(volatile int *)err)) {
         atomicExch(err, 1);
         break;
       }
