@@ -332,6 +332,31 @@ def roofline_fp64(ops, ms, peak, note):
             "work": note}
 
 
+def fp32_path_ops(n, nq):
+    """FP32-butterfly path, per X-string: (n + 2) 2^n FP32 ops (butterflies and the FP32
+    build of f) and (4 + 2 (nq - 1)) 2^n FP64 ops (the moment sums)."""
+    return float((n + 2) * (1 << n)), float((4 + 2 * (nq - 1)) * (1 << n))
+
+
+def roofline_fp32(ops32, ops64, ms, peak32, peak64):
+    """FP32 ops against the FP32 add peak, FP64 ops against the FP64 add peak; the pipe
+    whose work takes longer at its peak is the bound and gives the fraction."""
+    t32, t64 = ops32 / peak32, ops64 / peak64
+    f32, f64 = (ops32 / (ms * 1e-3)) / peak32, (ops64 / (ms * 1e-3)) / peak64
+    if t32 >= t64:
+        return {"bound": "fp32", "achieved": ops32 / (ms * 1e-3) / 1e12, "peak": peak32 / 1e12,
+                "unit": "Top/s (FP32 pipe)", "frac": f32, "traffic": None,
+                "peak_source": "measured live on this GPU: register-resident FADD kernel (hm_probe_fp32_peak)",
+                "work": "(n + 2) 2^n FP32 ops per X-string (butterflies, build); the FP64 moment sums "
+                        "(4 + 2 (nq - 1)) 2^n take less time at their peak",
+                "fp64_pipe_frac": f64}
+    return {"bound": "fp64", "achieved": ops64 / (ms * 1e-3) / 1e12, "peak": peak64 / 1e12,
+            "unit": "Top/s (FP64 pipe)", "frac": f64, "traffic": None,
+            "peak_source": "measured live on this GPU: register-resident DADD kernel (hm_probe_fp64_peak)",
+            "work": "(4 + 2 (nq - 1)) 2^n FP64 moment ops per X-string; the FP32 butterflies take less time",
+            "fp32_pipe_frac": f32}
+
+
 def base_line(args, cfg_name, metric, unit, value, world, total_ms, dtype, workload, extra_cfg):
     return {
         "metric": metric, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
@@ -392,9 +417,14 @@ def bench_sre(args, cfg, gpu, world, rank, dist):
 
     e2e_ms, _, _ = run_steps(argparse.Namespace(warmup=1, steps=args.steps), gpu, e2e_step, world, dist)
     my_ms = total_ms / args.steps
-    ops = fp64_ops_per_x(n, len(qs)) * float(ke - kb)
-    roof = roofline_fp64(ops, my_ms, gpu.ctx.probe_fp64_peak(),
-                         f"(n + 6 + 2 (nq - 1)) 2^n FP64 ops per X-string x {ke - kb} X-strings per step")
+    if precision == "fp32":
+        o32, o64 = fp32_path_ops(n, len(qs))
+        nx = float(ke - kb)
+        roof = roofline_fp32(o32 * nx, o64 * nx, my_ms, gpu.ctx.probe_fp32_peak(), gpu.ctx.probe_fp64_peak())
+    else:
+        ops = fp64_ops_per_x(n, len(qs)) * float(ke - kb)
+        roof = roofline_fp64(ops, my_ms, gpu.ctx.probe_fp64_peak(),
+                             f"(n + 6 + 2 (nq - 1)) 2^n FP64 ops per X-string x {ke - kb} X-strings per step")
     prof = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if os.path.exists(prof) and precision in json.load(open(prof)) and n == 20:
         d = json.load(open(prof))[precision]
@@ -503,9 +533,16 @@ def bench_batched(args, cfg, gpu, world, rank, dist):
     line["e2e"] = {"value": units_all * args.steps / (e2e_ms * 1e-3), "unit": "Pauli-strings*q/s",
                    "h2d_bytes_per_step": int(sum(16 * (1 << n) for n in ns)),
                    "d2h_bytes_per_step": int(8 * len(ns) * (len(qs) + 1))}
-    ops = sum(fp64_ops_per_x(n, len(qs)) * float(1 << n) for n in my_ns)
-    line["roofline"] = roofline_fp64(ops, total_ms / args.steps, gpu.ctx.probe_fp64_peak(),
-                                     "(n + 8) 2^n FP64 ops per X-string (q = 2 and 3), summed over the states")
+    if precision == "fp32":
+        o32 = sum(fp32_path_ops(n, len(qs))[0] * float(1 << n) for n in my_ns)
+        o64 = sum(fp32_path_ops(n, len(qs))[1] * float(1 << n) for n in my_ns)
+        line["roofline"] = roofline_fp32(o32, o64, total_ms / args.steps, gpu.ctx.probe_fp32_peak(),
+                                         gpu.ctx.probe_fp64_peak())
+        line["roofline"]["work"] += ", summed over the states"
+    else:
+        ops = sum(fp64_ops_per_x(n, len(qs)) * float(1 << n) for n in my_ns)
+        line["roofline"] = roofline_fp64(ops, total_ms / args.steps, gpu.ctx.probe_fp64_peak(),
+                                         "(n + 8) 2^n FP64 ops per X-string (q = 2 and 3), summed over the states")
     line["gpu_launches"] = int(launches)
     line["clocks"] = clocks
     if world == 1:

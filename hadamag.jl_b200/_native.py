@@ -32,7 +32,7 @@ EXPORTS = [
     "hm_abi_version", "hm_create", "hm_destroy", "hm_last_error", "hm_set_stream", "hm_last_kernel_ms",
     "hm_sre", "hm_sre_dev", "hm_sre_range", "hm_sre_range_dev", "hm_sre_batched", "hm_sre_grad",
     "hm_mc_sre", "hm_mana_pure", "hm_mana_mixed", "hm_gray_table", "hm_gray_table_general", "hm_set_param",
-    "hm_last_launch_count", "hm_probe_fp64_peak", "hm_sre_noalloc", "hm_autotune",
+    "hm_last_launch_count", "hm_probe_fp64_peak", "hm_probe_fp32_peak", "hm_sre_noalloc", "hm_autotune",
     "hm_apply_2gate", "hm_brick_wall", "hm_reduced_density_matrix", "hm_mc_sre_chains", "hm_mana_pure_range",
     "hm_sre_multi", "hm_sre_range_multi", "hm_multi_last_error", "hm_multi_release",
     "hm_load_state", "hm_free_state", "hm_io_last_error", "hm_gray_table_split", "hm_autotune_choice",
@@ -103,6 +103,7 @@ def load_library(path=None):
         L.hm_set_param.argtypes = [i, i]
         L.hm_last_launch_count.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong)]
         L.hm_probe_fp64_peak.argtypes = [_vp, _dp]
+        L.hm_probe_fp32_peak.argtypes = [_vp, _dp]
         L.hm_sre_noalloc.argtypes = [_dp, i, _dp, i, _dp, _dp, _vp]
         L.hm_autotune.argtypes = [_vp, i, i, _ip, _dp]
         L.hm_mc_sre_chains.argtypes = [_vp, _dp, i, d, i, i, i, i, _u64p, _dp, _dp, _dp, _dp, _u64p]
@@ -179,6 +180,11 @@ class Context:
     def probe_fp64_peak(self):
         v = ctypes.c_double()
         self._check(self.lib.hm_probe_fp64_peak(self.handle, ctypes.byref(v)), "hm_probe_fp64_peak")
+        return v.value
+
+    def probe_fp32_peak(self):
+        v = ctypes.c_double()
+        self._check(self.lib.hm_probe_fp32_peak(self.handle, ctypes.byref(v)), "hm_probe_fp32_peak")
         return v.value
 
     def autotune(self, n, precision=HM_FP64):

@@ -112,6 +112,22 @@ __global__ void k_probe_dadd(double *out, int iters, double s) {
   if (t == -1.0) out[0] = t;
 }
 
+// FP32 counterpart: 16 independent add chains per thread (the FP32 add latency is shorter
+// and its rate twice the FP64 rate, so more chains keep the pipe full)
+__global__ void k_probe_fadd(float *out, int iters, float s) {
+  float a[16];
+#pragma unroll
+  for (int j = 0; j < 16; ++j) a[j] = threadIdx.x + j;
+  for (int i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int j = 0; j < 16; ++j) a[j] = a[j] + s;
+  }
+  float t = 0.0f;
+#pragma unroll
+  for (int j = 0; j < 16; ++j) t += a[j];
+  if (t == -1.0f) out[0] = t;
+}
+
 }  // namespace
 
 extern "C" {
@@ -186,6 +202,24 @@ int hm_probe_fp64_peak(hm_ctx *c, double *ops_per_s) {
   float ms = 0.f;
   HM_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
   *ops_per_s = (double)blocks * threads * iters * 8.0 / (ms * 1e-3);
+  return HM_OK;
+}
+
+int hm_probe_fp32_peak(hm_ctx *c, double *ops_per_s) {
+  if (!c || !ops_per_s) return HM_ERR_ARG;
+  c->err.clear();
+  HM_CUDA(c, cudaSetDevice(c->device));
+  HM_TRY(ensure_dev(c, (void **)&c->d_out, &c->out_cap, sizeof(double) * 16));
+  const int blocks = c->num_sms * 8, threads = 256, iters = 8192;
+  k_probe_fadd<<<blocks, threads, 0, c->stream>>>((float *)c->d_out, 64, 1.0f);  // warm-up
+  HM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
+  k_probe_fadd<<<blocks, threads, 0, c->stream>>>((float *)c->d_out, iters, 1.0f);
+  HM_CUDA(c, cudaEventRecord(c->ev1, c->stream));
+  HM_CUDA(c, cudaGetLastError());
+  HM_CUDA(c, cudaEventSynchronize(c->ev1));
+  float ms = 0.f;
+  HM_CUDA(c, cudaEventElapsedTime(&ms, c->ev0, c->ev1));
+  *ops_per_s = (double)blocks * threads * iters * 16.0 / (ms * 1e-3);
   return HM_OK;
 }
 

@@ -127,6 +127,10 @@ int hm_last_launch_count(hm_ctx *ctx, long long *count);
  * reference counterpart. */
 int hm_probe_fp64_peak(hm_ctx *ctx, double *ops_per_s);
 
+/* The FP32 counterpart (register-resident FADD chains): FP32 add operations per second,
+ * the roofline of the FP32 butterflies of HM_FP32. */
+int hm_probe_fp32_peak(hm_ctx *ctx, double *ops_per_s);
+
 /* Device time in milliseconds of the main kernels of the last call (CUDA events on the
  * context's stream, recorded around the launches that do the transform work). */
 int hm_last_kernel_ms(hm_ctx *ctx, double *ms);
