@@ -26,6 +26,30 @@ __device__ __forceinline__ V v_sub(V a, V b) {
   r.y = a.y - b.y;
   return r;
 }
+#ifndef HM_NO_F32X2
+// FP32 complex values: one packed two-lane instruction (add/sub.rn.f32x2, sm_100) per
+// butterfly output instead of two; per lane the same round-to-nearest result as a + b.
+template <>
+__device__ __forceinline__ float2 v_add<float2>(float2 a, float2 b) {
+  unsigned long long ra, rb, rc;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(ra) : "f"(a.x), "f"(a.y));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(rb) : "f"(b.x), "f"(b.y));
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(rc) : "l"(ra), "l"(rb));
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(rc));
+  return r;
+}
+template <>
+__device__ __forceinline__ float2 v_sub<float2>(float2 a, float2 b) {
+  unsigned long long ra, rb, rc;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(ra) : "f"(a.x), "f"(a.y));
+  asm("mov.b64 %0, {%1, %2};" : "=l"(rb) : "f"(b.x), "f"(b.y));
+  asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(rc) : "l"(ra), "l"(rb));
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(rc));
+  return r;
+}
+#endif
 
 // Double-double accumulator (Knuth TwoSum on every addition).  Sums of partial
 // results land within ~1e-30 relative of the exact sum, so the final rounding to
