@@ -65,14 +65,15 @@ const char *hm_last_error(hm_ctx *ctx);
  * stream).  Lets a caller time the kernels with events on that stream. */
 int hm_set_stream(hm_ctx *ctx, void *cuda_stream);
 
-/* Tuning knobs of the exact-SRE two-pass sweep (n >= 12); the autotuner sets them,
- * defaults apply otherwise.  HM_PARAM_BATCH: X-strings per batch (1..4096; the
- * queue sweep rounds it down to a power of two; 0 = derive it from HM_PARAM_UNITS); HM_PARAM_RING: budget of the two-batch
- * intermediate ring in MiB (8..4096; it should stay L2 resident); HM_PARAM_UNITS: warp
- * units per pass the automatic batch size aims for (256..2^20); HM_PARAM_GRAPH: stage
- * kernels captured per CUDA graph (1..1024); HM_PARAM_ADJ_BATCH: X-strings per batch of
- * hm_sre_grad's stage kernels (power of two, 1..1024).  Value 0 restores the default.
- * Process-wide; returns HM_ERR_ARG for an unknown knob or value. */
+/* Tuning knobs of the exact-SRE multi-pass sweeps (n >= 12); the autotuner sets them,
+ * defaults apply otherwise.  HM_PARAM_BATCH: X-strings per batch (1..4096; the queue
+ * sweep rounds it down to a power of two; 0 = derive it from HM_PARAM_UNITS);
+ * HM_PARAM_RING: budget of the two-batch intermediate ring in MiB (8..4096; it should
+ * stay L2 resident); HM_PARAM_UNITS: warp units per pass the automatic batch size aims
+ * for (256..2^20); HM_PARAM_GRAPH: stage kernels captured per CUDA graph (1..1024,
+ * default 128; sweeps of at most 32 stages launch them directly); HM_PARAM_ADJ_BATCH:
+ * X-strings per batch of hm_sre_grad's stage kernels (power of two, 1..1024).  Value 0
+ * restores the default.  Process-wide; returns HM_ERR_ARG for an unknown knob or value. */
 #define HM_PARAM_BATCH 1
 #define HM_PARAM_RING 2
 #define HM_PARAM_UNITS 3
