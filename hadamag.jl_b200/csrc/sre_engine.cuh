@@ -402,14 +402,15 @@ __device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wa
 // As p1_unit, with the row leaving through the warp's shared buffer and tensor stores.
 // The caller waits for the stores to have read the buffer (bulk_wait_read_all on lane 0,
 // then __syncwarp) before the buffer's next use.
-template <int R, int HI, bool TM, typename V, typename Pre = NoHook>
+template <int R, int HI, bool TM, typename V, typename Pre = NoHook, typename Ready = NoHook>
 __device__ __forceinline__ void p1_unit_tma(const V *__restrict__ psi, const XInfo &xi, uint64_t rho, V *sm, int lane,
                                             const void *tmap, const TmaGeom &g, int xcoord, uint32_t ta,
-                                            const Pre &pre = Pre()) {
+                                            const Pre &pre = Pre(), const Ready &ready = Ready()) {
   constexpr int LOGR = ilog2c(R);
   V v[R];
-  p1_build<R, false>(v, psi, xi, rho, sm, lane);
+  p1_build<R, false>(v, psi, xi, rho, sm, lane);  // registers only (no shared memory)
   reg_wht<R, 0, LOGR>(v);
+  ready();  // the shared buffer is free from here on
 #ifdef HM_TMEM_EXCHANGE
   if constexpr (TM) {
     static_assert(R == 32, "the TMEM exchanges are generated for 32 values per lane");
@@ -439,9 +440,9 @@ __device__ __forceinline__ void p1_unit_tma(const V *__restrict__ psi, const XIn
 
 // Pass 2: tile of 2^HI rows x C = 2^(PB-HI) positions of one X-string's intermediate
 // (one contiguous block); transform over the row bits, then per-lane moments.
-template <int R, int HI, int QS, bool TM = false, typename V>
+template <int R, int HI, int QS, bool TM = false, typename V, typename Ready = NoHook>
 __device__ __forceinline__ void p2_unit(const V *__restrict__ tile_ptr, V *sm, int lane, double *s,
-                                        const QParams &qp, uint32_t ta = 0) {
+                                        const QParams &qp, uint32_t ta = 0, const Ready &ready = Ready()) {
   (void)ta;
   constexpr int LOGR = ilog2c(R), PB = LOGR + 5, LOGC = PB - HI;
   static_assert(HI >= 1 && HI <= PB, "pass-2 bits out of range");
@@ -450,14 +451,17 @@ __device__ __forceinline__ void p2_unit(const V *__restrict__ tile_ptr, V *sm, i
   for (int i = 0; i < R; ++i) v[i] = __ldcg(tile_ptr + i * 32 + lane);
   if constexpr (LOGC >= 5) {
     reg_wht<R, LOGC - 5, LOGR>(v);
+    ready();
 #ifdef HM_TMEM_EXCHANGE
   } else if constexpr (TM && R == 32) {
     reg_wht<R, 0, LOGR>(v);
+    ready();
     tmem_tile<HI>(v, ta);
     reg_wht<R, 0, 5 - LOGC>(v);
 #endif
   } else {
     reg_wht<R, 0, LOGR>(v);
+    ready();
     transpose_ab<R>(v, sm, lane);
     reg_wht<R, LOGC, 5>(v);
   }

@@ -190,21 +190,25 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
     V *inter_x = ring + ((size_t)(b & 1) * a.X + xs) * xlen;
     const XInfo xi = make_xinfo(k, a.k_end, n, PB);
     if (!xi.active) continue;
-    if (a.tma) {
-      // the previous unit's tensor stores must have read the shared buffer
-      if (lane == 0) bulk_wait_read_all();
-      __syncwarp();
-    }
+    // the previous unit's tensor stores must have read the shared buffer before this unit
+    // writes it: waited for right before the unit's first shared-memory access, so that
+    // the stores' read overlaps this unit's global loads and first butterflies
+    auto ready = [&] {
+      if (a.tma) {
+        if (lane == 0) bulk_wait_read_all();
+        __syncwarp();
+      }
+    };
     if (!p2) {
       const V *src = xi.sw < 0 ? psi : reinterpret_cast<const V *>(a.psi_sw[xi.sw]);
       if (a.tma)
-        p1_unit_tma<R, HI, TM>(src, xi, sub, sm, lane, &a.tmap, a.g, (int)((b & 1) * a.X + xs), ta, pre);
+        p1_unit_tma<R, HI, TM>(src, xi, sub, sm, lane, &a.tmap, a.g, (int)((b & 1) * a.X + xs), ta, pre, ready);
       else
         p1_unit<R, HI, false>(src, xi, sub, inter_x, sm, lane, pre);
     } else {
       double s[NQ + 1];
       wait_prior_grid();
-      p2_unit<R, HI, QS, TM>(inter_x + (sub << PB), sm, lane, s, a.qp, ta);
+      p2_unit<R, HI, QS, TM>(inter_x + (sub << PB), sm, lane, s, a.qp, ta, ready);
       // The tile is dead once read (its slot is rewritten by pass 1 two stages later, in
       // another launch): drop its L2 lines without writing them back to DRAM.  The next
       // write to the slot comes after griddepcontrol.wait on the launch in between, which

@@ -46,13 +46,14 @@ struct Stage3Args {
 };
 
 // pass 2 of the three-pass sweep: transform one tile over its 10 row bits, in place
-template <int R, typename V>
-__device__ __forceinline__ void p2_store_unit(V *tile, V *sm, int lane) {
+template <int R, typename V, typename Ready>
+__device__ __forceinline__ void p2_store_unit(V *tile, V *sm, int lane, const Ready &ready) {
   constexpr int LOGR = ilog2c(R);
   V v[R];
 #pragma unroll
   for (int i = 0; i < R; ++i) v[i] = __ldcg(tile + i * 32 + lane);
   reg_wht<R, 0, LOGR>(v);
+  ready();
   transpose_ab<R>(v, sm, lane);
   reg_wht<R, 0, 5>(v);
 #pragma unroll
@@ -61,9 +62,9 @@ __device__ __forceinline__ void p2_store_unit(V *tile, V *sm, int lane) {
 
 // pass 3: offsets [unit M, unit M + M) of every sub-vector (M = 32 R / 2^K); register
 // s J + j (J = R / 2^K) holds sub-vector s, offset unit M + 32 j + lane
-template <int R, int K, int QS, typename V>
+template <int R, int K, int QS, typename V, typename Ready>
 __device__ __forceinline__ void p3_unit(const V *x_base, uint64_t unit, V *sm, int lane, double *s,
-                                        const QParams &qp) {
+                                        const QParams &qp, const Ready &ready) {
   constexpr int LOGR = ilog2c(R), J = R >> K, M = (32 * R) >> K;
   const uint64_t m0 = unit * M;
   V v[R];
@@ -72,15 +73,17 @@ __device__ __forceinline__ void p3_unit(const V *x_base, uint64_t unit, V *sm, i
 #pragma unroll
     for (int j = 0; j < J; ++j) v[sv * J + j] = __ldcg(x_base + ((uint64_t)sv << 20) + m0 + j * 32 + lane);
   reg_wht<R, LOGR - K, LOGR>(v);  // the sub-vector bits
+  ready();
   lane_moments<R, QS>(v, s, qp, sm, lane);
 }
 
 // pass 1 of the three-pass sweep: row rho (n - 11 bits) of X-string k, stored into
 // sub-vector rho >> 10 at row rho & 1023, through tensor stores (tma) or plain stores
-template <int R, typename V, typename Pre>
+template <int R, typename V, typename Pre, typename Ready>
 __device__ __forceinline__ void p1_unit3(const V *__restrict__ psi, const V *__restrict__ src, uint64_t x, int n,
                                          uint64_t k, uint64_t k_end, uint64_t rho, V *sm, int lane, bool tma,
-                                         const void *tmap, const TmaGeom &g, int vx0, V *inter_x, const Pre &pre) {
+                                         const void *tmap, const TmaGeom &g, int vx0, V *inter_x, const Pre &pre,
+                                         const Ready &ready) {
   constexpr int LOGR = ilog2c(R), PB = LOGR + 5;
   V v[R];
   if (x == 0) {
@@ -94,9 +97,10 @@ __device__ __forceinline__ void p1_unit3(const V *__restrict__ psi, const V *__r
     }
   } else {
     const XInfo xi = make_xinfo(k, k_end, n, PB);
-    p1_build<R, false>(v, src, xi, rho, sm, lane);
+    p1_build<R, false>(v, src, xi, rho, sm, lane);  // registers only
   }
   reg_wht<R, 0, LOGR>(v);
+  ready();
   transpose_ab<R>(v, sm, lane);
   reg_wht<R, 0, 5>(v);
   const uint64_t sv = rho >> 10, rl = rho & 1023;
@@ -172,11 +176,14 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
     if (k >= a.k_end) continue;
     const int slotx = (int)(b % 3) * a.X + xs;
     V *inter_x = ring + (size_t)slotx * xlen;
-    if (a.tma) {
-      // the previous unit's tensor stores must have read the shared buffer
-      if (lane == 0) bulk_wait_read_all();
-      __syncwarp();
-    }
+    // the previous unit's tensor stores must have read the shared buffer before this unit
+    // writes it (waited for right before the unit's first shared-memory access)
+    auto ready = [&] {
+      if (a.tma) {
+        if (lane == 0) bulk_wait_read_all();
+        __syncwarp();
+      }
+    };
     if (pass == 1) {
       const uint64_t x = gray_code(k);
       int sw = -1;
@@ -185,14 +192,15 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
         if (jt < PB) sw = jt;
       }
       const V *src = sw < 0 ? psi : reinterpret_cast<const V *>(a.psi_sw[sw]);
-      p1_unit3<R>(psi, src, x, n, k, a.k_end, sub, sm, lane, a.tma != 0, &a.tmap, a.g, slotx << K, inter_x, pre);
+      p1_unit3<R>(psi, src, x, n, k, a.k_end, sub, sm, lane, a.tma != 0, &a.tmap, a.g, slotx << K, inter_x, pre,
+                  ready);
     } else if (pass == 2) {
       wait_prior_grid();
-      p2_store_unit<R>(inter_x + (sub << PB), sm, lane);
+      p2_store_unit<R>(inter_x + (sub << PB), sm, lane, ready);
     } else {
       wait_prior_grid();
       double s[NQ + 1];
-      p3_unit<R, K, QS>(inter_x, sub, sm, lane, s, a.qp);
+      p3_unit<R, K, QS>(inter_x, sub, sm, lane, s, a.qp, ready);
       // the lines are dead once read: the slot's next write is pass 1 of batch t + 1, in
       // the next launch, after its griddepcontrol.wait on this one
       {

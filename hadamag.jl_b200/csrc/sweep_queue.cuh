@@ -165,6 +165,17 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
   bool dirty = false;
   int si = 0;
   int pending = -1;  // batch whose pass-1 unit this warp finished but has not announced
+  // the warp's last tensor stores may still be reading its shared buffer: the next unit
+  // waits for them right before its first shared-memory access, so that the read overlaps
+  // that unit's global loads and first butterflies
+  bool sm_busy = false;
+  auto ready = [&]() {
+    if (sm_busy) {
+      if (lane == 0) bulk_wait_read_all();
+      __syncwarp();
+      sm_busy = false;
+    }
+  };
   long long u = 0, uend = 0;
 
   // announce the pending pass-1 unit once its tensor stores have completed (lane 0)
@@ -225,9 +236,6 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
     const long long p = u - s.u0;
     ++u;
     const int n = s.n;
-    // the previous unit's tensor stores must have read the shared buffer
-    if (lane == 0) bulk_wait_read_all();
-    __syncwarp();
     if (n <= 11) {
       // ---------------------------------------------------------------- fused unit
       const int NB = n - 1;
@@ -258,6 +266,7 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
         v[i].y = (T)f.y;
       }
       reg_wht_rt<R>(v, 0, NB - 5);
+      ready();
       transpose_ab<R>(v, sm, lane);
       reg_wht_rt<R>(v, 0, NB < 5 ? NB : 5);
       double sums[NQ + 1];
@@ -360,6 +369,7 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
           }
         }
         reg_wht<R, 0, 5>(v);
+        ready();
 #ifdef HM_TMEM_EXCHANGE
         tmem_row(v, ta);
 #else
@@ -381,6 +391,7 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
                              (int)sub, b2 * g.box2, xcoord);
             bulk_commit();
           }
+          sm_busy = true;
           pending = q;
         } else {
           // tile rows too narrow for a tensor map (FP32 at n = 21: 8 bytes): plain stores of
@@ -414,6 +425,7 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
           reg_wht_rt<R>(v, LOGC - 5, 5);
         } else {
           reg_wht<R, 0, 5>(v);
+          ready();
 #ifdef HM_TMEM_EXCHANGE
           switch (hi) {  // warp-uniform
             case 6: tmem_tile<6>(v, ta); break;
@@ -429,6 +441,7 @@ __global__ void __launch_bounds__(QWARPS * 32, QOcc<T>::value) k_sre_queue(const
 #endif
         }
         double sums[NQ + 1];
+        ready();  // the generic-q moments stage the values in the shared buffer
         lane_moments<R, QS>(v, sums, a.qp, sm, lane);
         const bool xz = gray_code(k) == 0;
         dd_add(acc[0], xz ? sums[0] : 4.0 * sums[0]);
