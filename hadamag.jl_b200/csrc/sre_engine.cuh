@@ -267,12 +267,14 @@ struct XInfo {
   int jt;       // pairing bit of xt
   int sw;       // relabelling: read the copy with bits sw and n-1 swapped (or -1)
   int active;   // Gray index inside the requested range and x != 0
+  int zero;     // x = 0 inside the range, built with the top-bit pairing (set by the caller)
 };
 
 __device__ __forceinline__ XInfo make_xinfo(uint64_t k, uint64_t k_end, int n, int pb) {
   XInfo xi;
   const uint64_t x = gray_code(k);
   xi.active = (k < k_end) && (x != 0);
+  xi.zero = 0;
   xi.sw = -1;
   xi.xt = x;
   xi.jt = x ? 63 - __clzll((long long)x) : n - 1;
@@ -310,6 +312,18 @@ template <int R, bool STAGE_B, typename V>
 __device__ __forceinline__ void p1_build(V (&v)[R], const V *__restrict__ psi, const XInfo &xi, uint64_t rho, V *sm,
                                          int lane) {
   constexpr int PB = ilog2c(R) + 5;
+  if (xi.zero) {
+    // x = 0: f(r) = |psi(r)|^2 paired on the top bit (jt = n - 1),
+    // h = (|a|^2 + |b|^2, |a|^2 - |b|^2) with a = psi(r), b = psi(r + 2^(n-1))
+    const V *rowA = psi + (rho << PB);
+    const V *rowB = rowA + (1ull << xi.jt);
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const uint32_t e = (uint32_t)(i * 32 + lane);
+      v[i] = zero_pair(ld_psi(rowA + e), ld_psi(rowB + e));
+    }
+    return;
+  }
   const uint64_t rH = insert0(rho, xi.jt - PB);
   const uint64_t sH = rH ^ (xi.xt >> PB);
   const uint32_t xL = (uint32_t)(xi.xt & ((1ull << PB) - 1ull));

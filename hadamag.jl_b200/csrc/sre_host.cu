@@ -205,12 +205,10 @@ int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, 
     HM_CUDA(c, cudaGetLastError());
     psi_k = c->d_psi32;
   }
-  // x = 0 (F = WHT of |psi|^2, whose F(0)^4 = 1 can dominate m) always runs in FP64: for
-  // 12 <= n <= 21 as one transform of the queue sweep (the two-pass stage kernels have no
-  // x = 0 build), for n >= 22 inside the three-pass kernels (an FP32 call runs it as an
-  // FP64 call of its own), and never in the FP32 kernels, which would round it
-  const bool three_pass = n >= 22;
-  const bool split_zero = kb == 0 && (three_pass ? precision == HM_FP32 : ((n - 1) > 10 || precision == HM_FP32));
+  // x = 0 (F = WHT of |psi|^2, whose F(0)^4 = 1 can dominate m) always runs in FP64: the
+  // FP64 kernels build it themselves (top-bit pairing in pass 1, scale 1), and an FP32 call
+  // runs it as an FP64 call of its own, since the FP32 kernels would round it
+  const bool split_zero = kb == 0 && precision == HM_FP32;
   const uint64_t kb_main = split_zero ? 1 : kb;
   int nwarps = 0;
   HM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
@@ -246,12 +244,7 @@ int run_sre(hm_ctx *c, const double2 *psi_dev, int n, uint64_t kb, uint64_t ke, 
     // transform of the queue sweep, added as a double-double term
     const double ms_main = c->last_ms;
     double z[10];
-    if (three_pass) {
-      HM_TRY(run_sre(c, psi_dev, n, 0, 1, q, HM_FP64, z));
-    } else {
-      const QueueItem zit{psi_dev, n, 0, 1};
-      HM_TRY(run_queue(c, &zit, 1, q, HM_FP64, z));
-    }
+    HM_TRY(run_sre(c, psi_dev, n, 0, 1, q, HM_FP64, z));
     c->last_ms += ms_main;
     for (int t = 0; t < 1 + q.nq; ++t) dd_add_host(out_dd + 2 * t, z[2 * t], z[2 * t + 1]);
   }

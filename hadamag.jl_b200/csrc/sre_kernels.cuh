@@ -188,8 +188,9 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
     const uint64_t sub = (uint64_t)(r / a.X);
     const uint64_t k = a.k_begin + (uint64_t)b * a.X + xs;
     V *inter_x = ring + ((size_t)(b & 1) * a.X + xs) * xlen;
-    const XInfo xi = make_xinfo(k, a.k_end, n, PB);
-    if (!xi.active) continue;
+    XInfo xi = make_xinfo(k, a.k_end, n, PB);
+    xi.zero = k < a.k_end && xi.xt == 0;  // x = 0 (Gray index 0): built with the top-bit pairing
+    if (!xi.active && !xi.zero) continue;
     // the previous unit's tensor stores must have read the shared buffer before this unit
     // writes it: waited for right before the unit's first shared-memory access, so that
     // the stores' read overlaps this unit's global loads and first butterflies
@@ -223,9 +224,9 @@ __global__ void __launch_bounds__(SRE_WARPS * 32, StageOcc<T>::value)
         for (int ln = lane; ln < LINES; ln += 32)
           asm volatile("discard.global.L2 [%0], 128;" ::"l"(tb + (size_t)ln * 128) : "memory");
       }
-      s[0] = 4.0 * s[0];
+      s[0] = xi.zero ? s[0] : 4.0 * s[0];  // the pairing scales: 4 and 4^q, 1 for x = 0
 #pragma unroll
-      for (int q = 0; q < NQ; ++q) s[1 + q] *= q_scale<QS>(q, false, a.qp);
+      for (int q = 0; q < NQ; ++q) s[1 + q] *= q_scale<QS>(q, xi.zero != 0, a.qp);
       if constexpr (LANE_ACC) {
         // per-lane double-double sums, reduced across the warp once per stage below
 #pragma unroll

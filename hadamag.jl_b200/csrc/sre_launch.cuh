@@ -186,7 +186,7 @@ static int launch_stages(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
     a.g = ring_tma_geom(C, NT);
     a.tma = encode_ring_tmap(&a.tmap, a.ring, (int)sizeof(T), C, 1 << HI, NT, 2 * (int)X, per_x, a.g) ? 1 : 0;
   }
-  if (a.k_begin < (1ull << PB)) {
+  if (a.k_begin < (1ull << PB) && a.k_end > 1) {  // some 0 < x < 2^PB in the range
     const size_t slen = (size_t)1 << a.n;
     HM_TRY(ensure_dev(c, &c->d_aux2, &c->aux2_cap, (size_t)PB * slen * sizeof(V)));
     k_psi_swapped<V><<<c->num_sms * 8, 256, 0, c->stream>>>(reinterpret_cast<const V *>(a.psi),
@@ -250,7 +250,7 @@ static int launch_stages3(hm_ctx *c, const SreArgs &a0, int *nwarps_out) {
                 ? 1
                 : 0;
   }
-  if (a.k_begin < (1ull << PB)) {
+  if (a.k_begin < (1ull << PB) && a.k_end > 1) {  // some 0 < x < 2^PB in the range
     const size_t slen = (size_t)1 << a.n;
     HM_TRY(ensure_dev(c, &c->d_aux2, &c->aux2_cap, (size_t)PB * slen * sizeof(V)));
     k_psi_swapped<V><<<c->num_sms * 8, 256, 0, c->stream>>>(reinterpret_cast<const V *>(a.psi),
