@@ -267,7 +267,7 @@ struct XInfo {
   int jt;       // pairing bit of xt
   int sw;       // relabelling: read the copy with bits sw and n-1 swapped (or -1)
   int active;   // Gray index inside the requested range and x != 0
-  int zero;     // x = 0 inside the range, built with the top-bit pairing (set by the caller)
+  int zero = 0;  // x = 0 inside the range, built with the top-bit pairing (set by the caller)
 };
 
 __device__ __forceinline__ XInfo make_xinfo(uint64_t k, uint64_t k_end, int n, int pb) {
