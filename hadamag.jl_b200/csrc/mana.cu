@@ -64,6 +64,13 @@ __device__ __forceinline__ void dft3(double2 &a, double2 &b, double2 &c) {
   c = make_double2(r2, i2);
 }
 
+// Consecutive Mana launches are chained by programmatic dependent launch: a grid lets the
+// next one be scheduled from its start, and every thread of the next grid waits for this
+// one to finish (and its memory to be visible) right before its first dependent access,
+// and in any case before it exits, so that a grid's completion implies its predecessors'.
+__device__ __forceinline__ void mana_allow_next() { asm volatile("griddepcontrol.launch_dependents;" :::); }
+__device__ __forceinline__ void mana_wait_prior() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __host__ __device__ constexpr int ipow3c(int e) { return e <= 0 ? 1 : 3 * ipow3c(e - 1); }
 
 // Register blocks of the qutrit transform H3^{(x)ND} of one vector of 3^ND elements
@@ -147,8 +154,12 @@ __global__ void __launch_bounds__(MANA_MAX_THREADS, 2) k_mana_p1(ManaArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   double2 *sm = reinterpret_cast<double2 *>(smraw);  // ROWS x VS (phase-B exchange)
   constexpr int VS = S::VS;
+  mana_allow_next();
   const int xi = blockIdx.y;
-  if (xi >= a.nx) return;  // uniform across the CTA
+  if (xi >= a.nx) {  // uniform across the CTA
+    mana_wait_prior();
+    return;
+  }
   const int x = a.x0 + xi;
   const int xL = x % RL, xH = x / RL;
   const int row0 = blockIdx.x * ROWS;
@@ -201,12 +212,18 @@ __global__ void __launch_bounds__(MANA_MAX_THREADS, 2) k_mana_p1(ManaArgs a) {
 #pragma unroll
         for (int m = 0; m < Q::MB; ++m) v[s * Q::MB + m] = sm[rr * VS + m + Q::MB * (t + T * s)];
       h3_regs<27, Q::B>(v);  // element digits 0 .. B-1
+    }
+    mana_wait_prior();  // the previous batch's pass 2 has read the intermediate
+    if (act) {
 #pragma unroll
       for (int r = 0; r < 27; ++r) out[r * T + t] = v[r];
     }
-  } else if (act) {
+  } else {
+    mana_wait_prior();
+    if (act) {
 #pragma unroll
-    for (int k = 0; k < E; ++k) out[k] = v[k];
+      for (int k = 0; k < E; ++k) out[k] = v[k];
+    }
   }
 }
 
@@ -227,6 +244,8 @@ __global__ void __launch_bounds__(MANA_MAX_THREADS, 2) k_mana_p2(ManaArgs a) {
   const bool act = xi < a.nx && t < T && c < ncols;
   const double2 *in = a.inter + (size_t)xi * RH * RL + c0 + c;
   double2 v[E];
+  mana_allow_next();
+  mana_wait_prior();  // pass 1 of this batch has stored the intermediate
   if (act) {
 #pragma unroll
     for (int k = 0; k < E; ++k) v[k] = in[(size_t)(t * E + k) * RL];
@@ -408,6 +427,24 @@ static M9 phase_point_matrix() {
 
 }  // namespace
 
+// one launch of a Mana pass, chained to the previous launch (chained = false for the
+// first launch of a call, which waits for everything before it)
+template <typename Kern>
+static int mana_launch(hm_ctx *c, Kern kern, dim3 grid, int threads, size_t smem, const ManaArgs &a, bool chained) {
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = grid;
+  lc.blockDim = dim3(threads);
+  lc.dynamicSmemBytes = smem;
+  lc.stream = c->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = at;
+  lc.numAttrs = chained ? 1 : 0;
+  HM_CUDA(c, cudaLaunchKernelEx(&lc, kern, a));
+  return HM_OK;
+}
+
 template <int LO, int HI>
 static int run_mana_pure_t(hm_ctx *c, const double2 *psi, int xb, int xe, double *sum_dd) {
   using S = ManaShape<LO, HI>;
@@ -443,8 +480,8 @@ static int run_mana_pure_t(hm_ctx *c, const double2 *psi, int xb, int xe, double
   for (int x0 = xb; x0 < xe; x0 += B) {
     a.x0 = x0;
     a.nx = std::min(B, xe - x0);
-    k1<<<dim3(g1, a.nx), S::NT1, S::SM1, c->stream>>>(a);
-    k2<<<dim3(g2, B), S::NT2, S::SM2, c->stream>>>(a);
+    HM_TRY(mana_launch(c, k1, dim3(g1, a.nx), S::NT1, S::SM1, a, x0 > xb));
+    HM_TRY(mana_launch(c, k2, dim3(g2, B), S::NT2, S::SM2, a, true));
     c->launches += 2;
   }
   HM_CUDA(c, cudaGetLastError());
