@@ -10,6 +10,7 @@
 // captured once as a CUDA graph and replayed.
 #include <math.h>
 
+#include <utility>
 #include <vector>
 
 #include "hm_ctx.h"
@@ -56,6 +57,8 @@ __global__ void __launch_bounds__(128) k_mc_fused(McArgs a) {
   constexpr int R = 32, LOGR = 5;
   extern __shared__ __align__(16) unsigned char smraw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  allow_next_grid();
+  wait_prior_grid();  // the previous update has written the proposals
   const int c = blockIdx.x * 4 + warp;
   if (c >= a.nbeta) return;
   double2 *sm = reinterpret_cast<double2 *>(smraw) + warp * 32 * R;
@@ -96,6 +99,8 @@ __global__ void __launch_bounds__(128) k_mc_p1(McArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double2 *sm = reinterpret_cast<double2 *>(smraw) + warp * 32 * R;
+  allow_next_grid();
+  wait_prior_grid();  // the previous update has written the proposals
   if (*a.step >= a.nsamples) return;
   const long long u = (long long)blockIdx.x * 4 + warp;
   if (u >= (long long)a.nbeta * a.U) return;
@@ -124,6 +129,8 @@ __global__ void __launch_bounds__(128) k_mc_p2(McArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   double2 *sm = reinterpret_cast<double2 *>(smraw) + warp * 32 * R;
+  allow_next_grid();
+  wait_prior_grid();  // pass 1 of this step has stored the rows
   if (*a.step >= a.nsamples) return;
   const long long u = (long long)blockIdx.x * 4 + warp;
   if (u >= (long long)a.nbeta * a.U) return;
@@ -150,6 +157,8 @@ __global__ void __launch_bounds__(128) k_mc_p2(McArgs a) {
 // nothing waits).
 constexpr int MC_UPD_WARPS = 4;
 __global__ void __launch_bounds__(MC_UPD_WARPS * 32) k_mc_update(McArgs a, int folded) {
+  allow_next_grid();
+  wait_prior_grid();  // this step's evaluation has finished
   const long long t = *a.step;
   const int c = blockIdx.x * MC_UPD_WARPS + (threadIdx.x >> 5), lane = threadIdx.x & 31;
   if (t < a.nsamples && c < a.nbeta) {
@@ -265,9 +274,31 @@ __global__ void k_mc_finish(McArgs a, double *out, uint64_t *final_mask) {
   out[0] = -log2(pow(2.0, -I_res) + I_add);
 }
 
+// One launch of a step kernel.  The kernels of consecutive steps are chained by
+// programmatic dependent launch (the next grid is set up while this one runs); every kernel
+// waits for its predecessor at its start, before any access to global memory, so the
+// order of their effects is the plain stream order.  The first launch of a captured block
+// is not chained: it waits for everything before it.
+template <typename... P, typename... A>
+static cudaError_t mc_launch(hm_ctx *c, bool chained, void (*kern)(P...), int blocks, int threads, size_t smem,
+                             A &&...args) {
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(blocks);
+  lc.blockDim = dim3(threads);
+  lc.dynamicSmemBytes = smem;
+  lc.stream = c->stream;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  lc.attrs = at;
+  lc.numAttrs = chained ? 1 : 0;
+  return cudaLaunchKernelEx(&lc, kern, std::forward<A>(args)...);
+}
+
 template <int QS>
-int mc_enqueue_step(hm_ctx *c, McArgs &a) {
+int mc_enqueue_step(hm_ctx *c, McArgs &a, bool first) {
   const int n = a.n;
+  const int upd_blocks = (a.nbeta + MC_UPD_WARPS - 1) / MC_UPD_WARPS;
   if (n <= 11) {
     const int nb = n - 1;
     const size_t smem = 4 * 32 * 32 * sizeof(double2);
@@ -276,7 +307,7 @@ int mc_enqueue_step(hm_ctx *c, McArgs &a) {
   case NBv:                                                                                     \
     HM_CUDA(c, cudaFuncSetAttribute(k_mc_fused<NBv, QS>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                     (int)smem));                                                \
-    k_mc_fused<NBv, QS><<<blocks, 128, smem, c->stream>>>(a);                                   \
+    HM_CUDA(c, mc_launch(c, !first, k_mc_fused<NBv, QS>, blocks, 128, smem, a));                 \
     break;
     switch (nb) {
       HM_MCF(0)
@@ -294,7 +325,7 @@ int mc_enqueue_step(hm_ctx *c, McArgs &a) {
         return set_err(c, HM_ERR_SIZE, "MC: n = %d", n);
     }
 #undef HM_MCF
-    k_mc_update<<<(a.nbeta + MC_UPD_WARPS - 1) / MC_UPD_WARPS, MC_UPD_WARPS * 32, 0, c->stream>>>(a, 0);
+    HM_CUDA(c, mc_launch(c, true, k_mc_update, upd_blocks, MC_UPD_WARPS * 32, 0, a, 0));
   } else {
     const int hi = n - 11;
     const size_t smem = 4 * 32 * 32 * sizeof(double2);
@@ -305,8 +336,8 @@ int mc_enqueue_step(hm_ctx *c, McArgs &a) {
     HM_CUDA(c, cudaFuncSetAttribute(k_mc_p1<HIv>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)); \
     HM_CUDA(c, cudaFuncSetAttribute(k_mc_p2<HIv, QS>, cudaFuncAttributeMaxDynamicSharedMemorySize,         \
                                     (int)smem));                                                           \
-    k_mc_p1<HIv><<<blocks, 128, smem, c->stream>>>(a);                                                  \
-    k_mc_p2<HIv, QS><<<blocks, 128, smem, c->stream>>>(a);                                              \
+    HM_CUDA(c, mc_launch(c, !first, k_mc_p1<HIv>, blocks, 128, smem, a));                               \
+    HM_CUDA(c, mc_launch(c, true, k_mc_p2<HIv, QS>, blocks, 128, smem, a));                             \
     break;
     switch (hi) {
       HM_MCP(1)
@@ -323,7 +354,7 @@ int mc_enqueue_step(hm_ctx *c, McArgs &a) {
         return set_err(c, HM_ERR_SIZE, "MC: n = %d outside [1, 21]", n);
     }
 #undef HM_MCP
-    k_mc_update<<<(a.nbeta + MC_UPD_WARPS - 1) / MC_UPD_WARPS, MC_UPD_WARPS * 32, 0, c->stream>>>(a, 1);
+    HM_CUDA(c, mc_launch(c, true, k_mc_update, upd_blocks, MC_UPD_WARPS * 32, 0, a, 1));
   }
   return HM_OK;
 }
@@ -381,7 +412,8 @@ int run_mc(hm_ctx *c, const double2 *psi, int n, double q, int nbeta_grid, int c
   HM_CUDA(c, cudaEventRecord(c->ev0, c->stream));
   HM_CUDA(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
   int rc = HM_OK;
-  for (int s = 0; s < G && rc == HM_OK; ++s) rc = q2 ? mc_enqueue_step<QS_Q2>(c, a) : mc_enqueue_step<QS_GEN>(c, a);
+  for (int s = 0; s < G && rc == HM_OK; ++s)
+    rc = q2 ? mc_enqueue_step<QS_Q2>(c, a, s == 0) : mc_enqueue_step<QS_GEN>(c, a, s == 0);
   cudaError_t ce = cudaStreamEndCapture(c->stream, &graph);
   if (rc != HM_OK) {
     if (graph) cudaGraphDestroy(graph);
