@@ -15,13 +15,15 @@ namespace hm {
 // outgrows the 126 MB L2 costs DRAM traffic.  Where they pull apart (n >= 18) the default
 // batch comes from `measured_x`, timed on B200 (us per X-string, stage kernels chained
 // by programmatic dependent launch, dead tiles discarded):
-//   FP64  n = 18: X = 32 (0.88)  n = 19: X = 16 (1.83; X = 4 1.94)
-//         n = 20: X = 8 (4.00; X = 16 4.18, X = 4 4.13)  n = 21: X = 2 (10.9; X = 8 22+)
-//   FP32  n = 18: X = 64 (0.49)  n = 19: X = 32 (1.05; X = 16 1.19)
-//         n = 20: X = 8 (2.91; X = 16 4.18)  n = 21: X = 4 (10.9)  hm_autotune measures and records a batch for the machine at
-// hand; setting HM_PARAM_BATCH, _UNITS or _RING switches to the generic rule.
+//   FP64  n = 18: X = 32 (0.95; X = 24 1.01)  n = 19: X = 16 (1.89; X = 12 1.91, X = 4 1.94)
+//         n = 20: X = 10 (3.86; X = 8 4.05, X = 12 3.91, X = 16 4.18)  n = 21: X = 2 (10.6; X = 3 14.5)
+//   FP32  n = 18: X = 64 (0.49)  n = 19: X = 32 (1.02; X = 16 1.09)
+//         n = 20: X = 8 (2.72; X = 10 2.74, X = 12 3.06)  n = 21: X = 2 (10.4; X = 4 11.2)
+// Any X works (the kernel decodes units with a division); larger rings than the L2 can
+// still win while the stage count falls.  hm_autotune measures and records a batch for the
+// machine at hand; setting HM_PARAM_BATCH, _UNITS or _RING switches to the generic rule.
 inline int measured_x(bool fp64, int n) {
-  static const int f64[4] = {32, 16, 8, 2}, f32[4] = {64, 32, 8, 4};
+  static const int f64[4] = {32, 16, 10, 2}, f32[4] = {64, 32, 8, 2};
   return (n >= 18 && n <= 21) ? (fp64 ? f64 : f32)[n - 18] : 0;
 }
 
