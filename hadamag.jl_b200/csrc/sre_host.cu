@@ -307,9 +307,16 @@ extern "C" int hm_autotune(hm_ctx *c, int n, int precision, int *best_x, double 
       if (rc == HM_OK && rep > 0) *t = std::min(*t, c->last_ms);
     }
   };
-  // stage kernels
+  // stage kernels: every power of two up to xmax and the sizes 1.25 and 1.5 times one
+  // (the kernel decodes its units with a division, so any X works; at n = 20 in FP64
+  // X = 10 beats both 8 and 16)
+  std::vector<uint64_t> xs;
+  for (uint64_t P = 1; P <= xmax; P *= 2)
+    for (uint64_t X : {P, P + P / 4, P + P / 2})
+      if (X <= xmax && (xs.empty() || X > xs.back())) xs.push_back(X);
   qc.engine = 1;
-  for (uint64_t X = 1; X <= xmax && rc == HM_OK; X *= 2) {
+  for (size_t xi = 0; xi < xs.size() && rc == HM_OK; ++xi) {
+    const uint64_t X = xs[xi];
     cfg.X = (int)X;
     cfg.X_set = 1;
     cfg.ring_mib = std::max<int>(saved.ring_mib, (int)((2 * X * per_x + (1 << 20) - 1) >> 20));

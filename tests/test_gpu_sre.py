@@ -138,7 +138,7 @@ def test_autotune_records_a_batch_size(ctx, hm, oracle):
     ref = oracle.sre(psi, 2)[0]
     for prec in ("fp64", "fp32"):
         x, us = ctx.autotune(n, hm.PRECISIONS[prec])
-        assert x >= 1 and (x & (x - 1)) == 0 and us > 0
+        assert x >= 1 and us > 0  # the stage kernels take any batch size, the queue a power of two
         eng, bx, cps = hm._native.autotune_choice(n, hm.PRECISIONS[prec])
         assert eng in (1, 2) and bx == x and cps in (0, 1)
         v, _ = ctx.sre(psi, (2.0,), hm.PRECISIONS[prec])  # runs with the tuned engine and batch size
