@@ -108,8 +108,9 @@ int hm_set_stream(hm_ctx *ctx, void *cuda_stream);
 int hm_set_param(int param, int value);
 
 /* Autotuner of the two-pass sweep (no reference counterpart): times the sweep of an n-qubit
- * state on a sample of Gray indices with the stage kernels (X = 1, 2, 4, ... X-strings per
- * stage) and with the queue sweep (X = 1, 2, 4, ... X-strings per ring slot, at full
+ * state on a sample of Gray indices with the stage kernels (X = 1, 2, 3, 4, 5, 6, 8, 10,
+ * 12, ... X-strings per stage: each power of two and 1.25 and 1.5 times it) and with the
+ * queue sweep (X = 1, 2, 4, ... X-strings per ring slot, at full
  * occupancy and at one CTA per SM), records the fastest engine, batch size and CTAs per
  * SM for this (n, precision) in a process-wide table that later calls use unless a knob
  * forces another choice, and returns the batch size with the measured microseconds per
